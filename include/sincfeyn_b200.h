@@ -1,0 +1,109 @@
+/* sincfeyn_b200.h -- the C ABI of the B200 evaluator for sincFeyn's hierarchical Sinc sum.
+ *
+ * Two forms share one shared library, libsqb200.so:
+ *
+ * 1. The plain form: the reference's GPU plug-in ABI, unchanged (driver/gpu.h:12-22).  The reference
+ *    driver built with -DSQ_GPU (driver/eval.c:97-203, driver/lattice.c:20-22) links against this library
+ *    instead of its own driver/gpu.cu and evaluates every batch with this library's sm_100a kernels.
+ *
+ * 2. The chosen form: one call per integral, sqb_hsum(), which replaces the body of the reference's
+ *    hsum() (driver/sum.c:556-814): the top level on the host, every refinement level resident on the
+ *    device (FP64 bulk, double-double only for the points the reference's fallback test flags,
+ *    double-double level sums), with the same results structure as res_t (driver/sq.h:111).
+ *
+ * All pointers are host pointers unless a comment says device.  No function here exits the process
+ * except where the reference's plug-in contract does (CUDA errors and a D mismatch in the plain form,
+ * driver/gpu.cu:16,59); the chosen form returns an error code and sqb_error() says why. */
+#pragma once
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------------------
+ * 1. Plain form: the reference's GPU plug-in (replaces driver/gpu.cu; declarations as driver/gpu.h)
+ * ------------------------------------------------------------------------------------------------ */
+#ifdef __CUDACC__
+typedef cudaStream_t sq_stream_t;
+#else
+typedef void *sq_stream_t;
+#endif
+/* launcher of one graph's batch kernel on device buffers (driver/gpu.h:17-19) */
+typedef void (*sq_gpu_launch_t)(sq_stream_t st, long n, const short *k, const unsigned char *skip,
+                                const double *EX, int K, double H, double *of, double *oab, int cmode, int cst);
+typedef struct { const char *name; int D; sq_gpu_launch_t launch; } sq_gpu_t;   /* driver/gpu.h:20 */
+extern const sq_gpu_t *GPU_ALL[];            /* NULL-terminated, one GG_<name> per graph (Makefile:231-234) */
+
+/* driver/gpu.h:23: 1 if this graph has a GPU kernel (then D must match, else exit(3)), 0 = CPU path */
+int  gpu_setup(const char *name, int D, const double *EX, int K, double H);
+/* driver/gpu.h:24: n nodes k[i*stride + d]; skip (may be NULL) per node; returns at once */
+void gpu_submit(int slot, long n, const int *k, int stride, const unsigned char *skip);
+/* driver/gpu.h:25: waits for the slot; fw = f*w, abw = sum|terms|*w, valid until the slot's next submit */
+void gpu_wait(int slot, const double **fw, const double **abw);
+/* driver/gpu.h:27: the 2^D children of nc cells at step st; nc << D results in prep() order */
+void gpu_submit_cells(int slot, long nc, const int *cells, int stride, const unsigned char *skip, int st);
+/* driver/gpu.h:28 */
+const char *gpu_info(void);
+
+/* ------------------------------------------------------------------------------------------------
+ * 2. Chosen form
+ * ------------------------------------------------------------------------------------------------ */
+/* the run parameters that the reference reads from its environment (driver/main.c:176-185,
+ * driver/eval.c:7-24); sqb_default_opts() gives the reference's defaults */
+typedef struct {
+    double abserr0;        /* G2_ABSERR: floor of the per-point fallback threshold (1e-15) */
+    double abrel;          /* SINCQED_ABREL: ABSERR = max(abserr0, abrel*eps*Ref) in the levels (1e-3) */
+    double nearf;          /* SINCQED_NEARF (1e-3) */
+    double ddslack;        /* SINCQED_DDSLACK (1) */
+    int abskip;            /* SINCQED_ABSKIP (1) */
+    int abcheck;           /* SINCQED_ABCHECK (0) */
+    int dropunres;         /* SINCQED_DROPUNRES (1) */
+    int growskip;          /* SINCQED_GROWSKIP, top = 0 only (2) */
+    int alldd;             /* 1: every point in double-double (the plain all-dd form); 0: FP64 + fallback */
+    int device;            /* CUDA device (0) */
+    long max_children;     /* children per device batch, 0 = default (2^25) */
+    int verbose;           /* 1: timing lines on stderr */
+} sqb_opts_t;
+
+/* res_t of the reference (driver/sq.h:111) and the per-graph log counters (driver/main.c:58-65) */
+typedef struct {
+    double S[3];           /* S_h, S_2h, S_4h (NaN where the run had no such level) */
+    double Ah, ref, prune, trunc, unres, t;
+    long nev, nq, kept_top;
+    double es1, es2;       /* shadow-tier sums at the last level (eps*10, eps*100 runs) */
+    int esok;
+    long abskipped, unresdrop;
+    int zero;              /* the integrand vanished at every probe node (driver/sum.c:346-359) */
+    /* timing: host seconds for the top level (grow + dilate), device milliseconds per level */
+    double t_top, t_levels;
+    int nlev;
+    long lev_evals[16];
+    double lev_ms[16];
+} sqb_result_t;
+
+void sqb_default_opts(sqb_opts_t *o);
+/* the hierarchical Sinc sum of one graph at (h, N, eps, top); top < 0 picks the reference's default
+ * (driver/main.c:211-215).  Returns 0, or a nonzero error code (sqb_error() has the message). */
+int  sqb_hsum(const char *graph, double h, int N, double eps, int top, const sqb_opts_t *o, sqb_result_t *r);
+const char *sqb_error(void);
+
+/* the graphs compiled into this library: name, Volkov string, L, D, mirror weight */
+int  sqb_graph_count(void);
+const char *sqb_graph_name(int i);
+/* info[0..5] = L, D, weight, n, fixed, zlattice; returns 0 if unknown */
+int  sqb_graph_info(const char *name, int *info);
+const char *sqb_graph_volkov(const char *name);
+/* algorithmic FP64 flops per point of the graph's double path, with (ab=1) or without (ab=0) the |.|
+ * sums: + - * / counted 1 each (scripts/plot5_cost.py:11); 0 if unknown */
+double sqb_graph_flops(const char *name, int ab);
+
+/* pointwise evaluation of the graph kernels on the device, for parity checks: n points sf[i*D + d]
+ * (the Sinc variables), outputs f and the |.| sum; prec 0 = FP64 (ab: SQ_AB), 1 = double-double,
+ * returned as (hi, lo) pairs in f2 and ab2 (2n entries each) */
+int  sqb_eval_points(const char *graph, long n, const double *sf, int prec, int ab, double *f, double *abs_);
+
+/* the device the library runs on ("off" before the first call) */
+const char *sqb_device_info(void);
+
+#ifdef __cplusplus
+}
+#endif

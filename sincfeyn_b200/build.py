@@ -1,0 +1,227 @@
+"""Build of the evaluator: generated per-graph CUDA, the runtime, the C-ABI library and the CLI.
+
+    python -m sincfeyn_b200.build [--kernels DIR] [--classes "g2 g3 v3"] [-j N]
+
+Inputs are the generated sincFeyn kernel sources (kernels/<class>/<g>.c of the reference tree, the same
+files its tools/gpugen.py reads).  Outputs, all in-tree and git-ignored:
+  sincfeyn_b200/_build/gen/   kgen output (<g>.cuh), the per-graph translation units, the registry;
+  sincfeyn_b200/_build/obj/   objects;
+  sincfeyn_b200/lib/libsqb200.so   the C ABI (include/sincfeyn_b200.h), every graph's sm_100a kernels;
+  sincfeyn_b200/bin/sincqed        the command line;
+  sincfeyn_b200/lib/flops.json     algorithmic FP64 flops per point of every graph (SQ_AB = 1 and 0).
+A step is redone only when one of its inputs is newer than its output.  Without a kernel tree (e.g. on
+a host that only runs the prebuilt library) the build keeps what is there.
+"""
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+
+from .codegen import kgen
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, 'csrc')
+BUILD = os.path.join(PKG, '_build')
+GEN = os.path.join(BUILD, 'gen')
+OBJ = os.path.join(BUILD, 'obj')
+LIB = os.path.join(PKG, 'lib')
+BIN = os.path.join(PKG, 'bin')
+INC = os.path.join(ROOT, 'include')
+DEFAULT_KERNELS = os.environ.get('SQB_KERNELS', '/root/reference/kernels')
+DEFAULT_CLASSES = os.environ.get('SQB_CLASSES', 'g2 g3 v3')
+
+NVCC = os.environ.get('NVCC', 'nvcc')
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+# -fmad=false: the kernels' cancellations must round as written (no contraction), exactly as the
+# reference CPU code compiled without contraction; the double-double code uses explicit intrinsics.
+NVFLAGS = ARCH + ['-O3', '-lineinfo', '-fmad=false', '-std=c++17', '-Xcompiler', '-fPIC',
+                  '-diag-suppress', '177,550', '-I' + CSRC, '-I' + INC]
+CXX = 'g++'   # the system compiler (an environment CXX may lack libgomp.spec)
+CXXFLAGS = ['-O2', '-fPIC', '-fopenmp', '-std=c++17', '-I' + CSRC, '-I' + INC, '-I/usr/local/cuda/include']
+
+LIBSO = os.path.join(LIB, 'libsqb200.so')
+CLI = os.path.join(BIN, 'sincqed')
+FLOPS = os.path.join(LIB, 'flops.json')
+
+
+def _newer(out, ins):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(i) > t for i in ins if os.path.exists(i))
+
+
+def _run(cmd, log=None):
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode:
+        raise RuntimeError('build step failed (%d): %s\n%s' % (r.returncode, ' '.join(cmd), r.stdout[-4000:]))
+    return r.stdout
+
+
+def kernel_sources(kdir, classes):
+    out = []
+    for c in classes.split():
+        d = os.path.join(kdir, c)
+        if os.path.isdir(d):
+            out += sorted(os.path.join(d, f) for f in os.listdir(d) if f.endswith('.c'))
+    return out
+
+
+def generate(srcs):
+    """kgen every kernel; returns [(name, D, cuh path, tu path)] in registry order (first name wins,
+    as driver/graphs.c:8-12)."""
+    os.makedirs(GEN, exist_ok=True)
+    me = [os.path.abspath(kgen.__file__)]
+    graphs, seen = [], set()
+    for src in srcs:
+        base = os.path.splitext(os.path.basename(src))[0]
+        cuh = os.path.join(GEN, base + '.cuh')
+        if _newer(cuh, [src] + me):
+            k, text = kgen.emit(src)
+            with open(cuh, 'w') as f:
+                f.write(text)
+        with open(cuh) as f:
+            m = re.search(r'^SQ_GRAPH\((\w+), "((?:[^"\\]|\\.)*)", (\d+), (\d+),', f.read(), re.M)
+        name, D = m.group(1), int(m.group(4))
+        if name in seen:
+            continue
+        seen.add(name)
+        tu = os.path.join(GEN, 'k_%s.cu' % name)
+        text = '#include "sqkern.cuh"\n#include "%s"\n' % os.path.basename(cuh)
+        if not os.path.exists(tu) or open(tu).read() != text:
+            with open(tu, 'w') as f:
+                f.write(text)
+        graphs.append((name, D, cuh, tu))
+    return graphs
+
+
+def write_registry(graphs, flops):
+    reg = os.path.join(GEN, 'registry.cu')
+    L = ['/* generated by sincfeyn_b200/build.py: the graphs of this library */',
+         '#include "sqb_internal.h"', '#include "sincfeyn_b200.h"', '#include <string.h>']
+    for name, D, _, _ in graphs:
+        L.append('extern "C" const sqb_graph_t SQB_%s;' % name)
+    L.append('extern "C" const sqb_graph_t *const SQB_ALL[] = {')
+    L += ['    &SQB_%s,' % n for n, _, _, _ in graphs] + ['    0 };', 'extern "C" const int SQB_NALL = %d;' % len(graphs)]
+    # the reference's per-graph plug-in descriptors GG_<name> (driver/gpu_kernel.h:39, Makefile:231-234)
+    L.append('extern "C" void sqb_gg_launch(const sqb_graph_t *g, void *st, long n, const short *k, const unsigned char *skip,'
+             ' const double *EX, int K, double H, double *of, double *oab, int cmode, int cst);')
+    for name, D, _, _ in graphs:
+        L.append('static void gl_%s(sq_stream_t st, long n, const short *k, const unsigned char *skip, const double *EX, int K,'
+                 ' double H, double *of, double *oab, int cmode, int cst){ sqb_gg_launch(&SQB_%s, (void*)st, n, k, skip, EX, K, H,'
+                 ' of, oab, cmode, cst); }' % (name, name))
+        L.append('extern "C" const sq_gpu_t GG_%s = {"%s", %d, gl_%s};' % (name, name, D, name))
+    L.append('extern "C" const sq_gpu_t *GPU_ALL[] = {')
+    L += ['    &GG_%s,' % n for n, _, _, _ in graphs] + ['    0 };']
+    L.append('static const struct { const char *name; double ab1, ab0; } FLOPS[] = {')
+    for name, _, _, _ in graphs:
+        f = flops.get(name, {})
+        L.append('    {"%s", %.1f, %.1f},' % (name, f.get('ab1', 0), f.get('ab0', 0)))
+    L += ['    {0, 0, 0} };',
+          'extern "C" double sqb_graph_flops(const char *name, int ab){',
+          '    for(int i = 0; FLOPS[i].name; i++) if(!strcmp(FLOPS[i].name, name)) return ab ? FLOPS[i].ab1 : FLOPS[i].ab0;',
+          '    return 0; }']
+    text = '\n'.join(L) + '\n'
+    if not os.path.exists(reg) or open(reg).read() != text:
+        with open(reg, 'w') as f:
+            f.write(text)
+    return reg
+
+
+def count_flops(graphs):
+    """Compile every generated kernel over the counting type on the host and count one point."""
+    src = os.path.join(GEN, 'count.cc')
+    exe = os.path.join(BUILD, 'count')
+    L = ['/* generated by sincfeyn_b200/build.py: algorithmic flop counter */',
+         '#include <stdio.h>', '#include "sqcount.h"', 'long sq_flops;',
+         '#define SQ_TABLE static const', '#define SQ_FUNC', '#define SQ_CHUNK', '#define RABS(x) sq_rabs(x)',
+         '#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX) \\',
+         'static void count_##NAME(void){ sq_count sf[D], ab; for(int d = 0; d < D; d++) sf[d] = sq_count(0.7 + 0.37*d); \\',
+         '  sq_flops = 0; sqg_##NAME::K<sq_count, 1>::f_##NAME(sf, &ab); long a1 = sq_flops; \\',
+         '  sq_flops = 0; sqg_##NAME::K<sq_count, 0>::f_##NAME(sf, &ab); long a0 = sq_flops; \\',
+         '  printf("%s\\"%s\\": {\\"ab1\\": %ld, \\"ab0\\": %ld}", first ? "" : ",\\n", #NAME, a1, a0); first = 0; }',
+         'static int first = 1;']
+    for name, D, cuh, _ in graphs:
+        L.append('#include "%s"' % os.path.basename(cuh))
+    L.append('int main(void){ printf("{\\n");')
+    L += ['  count_%s();' % n for n, _, _, _ in graphs]
+    L.append('  printf("\\n}\\n"); return 0; }')
+    text = '\n'.join(L) + '\n'
+    if not os.path.exists(src) or open(src).read() != text:
+        with open(src, 'w') as f:
+            f.write(text)
+    if _newer(exe, [src, os.path.join(CSRC, 'sqcount.h')] + [g[2] for g in graphs]):
+        _run([CXX, '-O0', '-std=c++17', '-I' + CSRC, '-I' + GEN, '-o', exe, src])
+    if _newer(FLOPS, [exe]):
+        out = _run([exe])
+        os.makedirs(LIB, exist_ok=True)
+        with open(FLOPS, 'w') as f:
+            f.write(out)
+    with open(FLOPS) as f:
+        return json.load(f)
+
+
+def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=True):
+    """Generate and compile whatever is out of date; returns the library path."""
+    srcs = kernel_sources(kernels, classes)
+    if not srcs:
+        if os.path.exists(LIBSO):
+            return LIBSO
+        raise RuntimeError('no kernel sources under %s and no prebuilt %s' % (kernels, LIBSO))
+    os.makedirs(OBJ, exist_ok=True)
+    os.makedirs(LIB, exist_ok=True)
+    os.makedirs(BIN, exist_ok=True)
+    graphs = generate(srcs)
+    flops = count_flops(graphs)
+    reg = write_registry(graphs, flops)
+    hdrs = [os.path.join(CSRC, f) for f in ('sqkern.cuh', 'sqdd.cuh', 'sqb_internal.h', 'sqb_rt.h')] + \
+           [os.path.join(INC, 'sincfeyn_b200.h')]
+    jobs_list = []
+    for name, D, cuh, tu in graphs:
+        o = os.path.join(OBJ, 'k_%s.o' % name)
+        if _newer(o, [tu, cuh] + hdrs):
+            jobs_list.append([NVCC] + NVFLAGS + ['-I' + GEN, '-c', tu, '-o', o])
+    rt_o = os.path.join(OBJ, 'runtime.o')
+    if _newer(rt_o, [os.path.join(CSRC, 'runtime.cu')] + hdrs):
+        jobs_list.append([NVCC] + NVFLAGS + ['-Xcompiler', '-fopenmp', '-c', os.path.join(CSRC, 'runtime.cu'), '-o', rt_o])
+    reg_o = os.path.join(OBJ, 'registry.o')
+    if _newer(reg_o, [reg] + hdrs):
+        jobs_list.append([NVCC] + NVFLAGS + ['-c', reg, '-o', reg_o])
+    eng_o = os.path.join(OBJ, 'engine.o')
+    if _newer(eng_o, [os.path.join(CSRC, 'engine.cpp')] + hdrs):
+        jobs_list.append([CXX] + CXXFLAGS + ['-c', os.path.join(CSRC, 'engine.cpp'), '-o', eng_o])
+    n = jobs or min(len(jobs_list) or 1, os.cpu_count() or 4)
+    if verbose and jobs_list:
+        print('sincfeyn_b200: compiling %d objects with %d jobs' % (len(jobs_list), n), file=sys.stderr)
+    with cf.ThreadPoolExecutor(max_workers=n) as ex:
+        for f in [ex.submit(_run, c) for c in jobs_list]:
+            f.result()
+    objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + [rt_o, reg_o, eng_o]
+    if _newer(LIBSO, objs):
+        _run([NVCC] + ARCH + ['-shared', '-o', LIBSO] + objs + ['-Xcompiler', '-fopenmp', '-lgomp'])
+    main_cpp = os.path.join(CSRC, 'main.cpp')
+    if _newer(CLI, [main_cpp, LIBSO, os.path.join(INC, 'sincfeyn_b200.h')]):
+        _run([CXX, '-O2', '-std=c++17', '-I' + INC, '-o', CLI, main_cpp, '-L' + LIB, '-lsqb200',
+              '-Wl,-rpath,$ORIGIN/../lib'])
+    return LIBSO
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument('--kernels', default=DEFAULT_KERNELS)
+    ap.add_argument('--classes', default=DEFAULT_CLASSES)
+    ap.add_argument('-j', '--jobs', type=int, default=None)
+    ap.add_argument('--clean', action='store_true')
+    a = ap.parse_args(argv)
+    if a.clean:
+        shutil.rmtree(BUILD, ignore_errors=True)
+    print(build(a.kernels, a.classes, a.jobs))
+
+
+if __name__ == '__main__':
+    main()

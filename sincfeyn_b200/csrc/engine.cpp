@@ -1,0 +1,343 @@
+/* engine.cpp -- the host side of the chosen form: sqb_hsum(), the hierarchical Sinc sum of one graph
+ * (driver/sum.c:556-814), with every refinement level resident on the device.
+ *
+ *   lattice      K rounded up to a multiple of 2^(top+1); EX[k+K] = e^{kh}, weight factor EX*h
+ *                (driver/lattice.c:13-34);
+ *   box_zero     4097 fixed probe nodes; an integrand that is 0 at all of them is reported as zero
+ *                (driver/sum.c:346-359);
+ *   grow         the support-following top level (driver/sumkey.h:126-461): breadth-first from z = 0
+ *                over axis neighbours at step 2^top h; a frontier is evaluated as one device batch;
+ *                the running threshold eps_rel * sum|f w|; the next frontier is every not-yet-seen
+ *                neighbour of a kept point, in (kept point, axis, sign) order -- the order the
+ *                reference's parallel lowest-id claims produce; then the final re-threshold and the
+ *                shadow-tier flood fill.  One table holds every evaluated point, which is the
+ *                reference's result whenever it reports no candidate below its freed boundary
+ *                tables (BTUNS = 0, driver/sum.c:631);
+ *   dilate       the kept cells and their axis neighbours, deduplicated (skip bit AND, tier max) and
+ *                sorted by mixed-radix key, i.e. lexicographically in k (driver/sumkey.h:20-90);
+ *   levels       sqb_dev_level() for lev = top-1 .. 0 (driver/sum.c:652-799), the cell lists staying
+ *                in device memory.
+ * Sums of the grow are Neumaier sums in point order as the reference's kadd (driver/sum.c:18-20);
+ * the levels' sums are double-double on the device. */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include <stdint.h>
+#include <vector>
+#include <algorithm>
+#include <omp.h>
+#include <chrono>
+#include "sqb_rt.h"
+#include "sincfeyn_b200.h"
+
+static char E_[512];
+extern "C" const char *sqb_error(void){ return E_; }
+#define FAIL(...) do { snprintf(E_, sizeof E_, __VA_ARGS__); return -1; } while(0)
+
+static double now(void){ return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+
+extern "C" void sqb_default_opts(sqb_opts_t *o){
+    memset(o, 0, sizeof *o);
+    o->abserr0 = 1e-15; o->abrel = 1e-3; o->nearf = 1e-3; o->ddslack = 1;
+    o->abskip = 1; o->abcheck = 0; o->dropunres = 1; o->growskip = 2;
+    o->alldd = 0; o->device = 0; o->max_children = 0; o->verbose = 0;
+}
+
+extern "C" int sqb_graph_count(void){ return sqb_ngraphs(); }
+extern "C" const char *sqb_graph_name(int i){ const sqb_graph_t *g = sqb_graph_at(i); return g ? g->name : NULL; }
+extern "C" const char *sqb_graph_volkov(const char *name){ const sqb_graph_t *g = sqb_find_graph(name); return g ? g->volkov : NULL; }
+extern "C" int sqb_graph_info(const char *name, int *info){
+    const sqb_graph_t *g = sqb_find_graph(name); if(!g) return 0;
+    info[0] = g->L; info[1] = g->D; info[2] = g->weight; info[3] = g->n; info[4] = g->fixed; info[5] = g->zlattice;
+    return 1;
+}
+extern "C" const char *sqb_device_info(void){ return sqb_dev_info(); }
+
+/* Neumaier sum, driver/sum.c:18-20 */
+struct ksum { double s = 0, c = 0;
+    void add(double x){ double t = s + x; if(fabs(s) >= fabs(x)) c += (s - t) + x; else c += (x - t) + s; s = t; }
+    double val() const { return s + c; } };
+
+/* ---------------------------------------------------------------------------------------------- */
+/* the run of one graph */
+struct Run {
+    const sqb_graph_t *g; int D, K, top; double h, eps;
+    sqb_opts_t o; sqb_test_t t;
+    std::vector<double> X, Wt;
+    long nq = 0, unresdrop = 0; double u = 0;
+};
+
+static void set_test(Run &R, double abserr){
+    R.t.abserr = abserr; R.t.nearf = R.o.nearf; R.t.ddslack = R.o.ddslack;
+    R.t.abskip = R.o.abskip; R.t.abcheck = R.o.abcheck; R.t.dropunres = R.o.dropunres; R.t.alldd = R.o.alldd;
+}
+
+static int eval(Run &R, const std::vector<sqb_pt_t> &p, const unsigned char *skip, std::vector<double> &v, std::vector<unsigned char> &nr){
+    v.resize(p.size()); nr.resize(p.size());
+    if(p.empty()) return 0;
+    if(sqb_dev_eval_nodes(R.g, (long)p.size(), p.data(), skip, &R.t, v.data(), nr.data(), &R.nq, &R.u, &R.unresdrop))
+        FAIL("device: %s", sqb_last_error());
+    return 0;
+}
+
+/* driver/sum.c:346-359 */
+static int box_zero(Run &R, int lev, long *nev, int *zero){
+    const int st = 1 << lev, W = 2*(R.K/st) + 1, NP = 4096;
+    std::vector<sqb_pt_t> p(NP + 1);
+    for(long i = 0; i <= NP; i++){
+        memset(&p[i], 0, sizeof p[i]);
+        unsigned long long y = 0x9E3779B97F4A7C15ULL*(unsigned long long)(i + 1);
+        if(i) for(int d = 0; d < R.D; d++){ y ^= y >> 29; y *= 0xBF58476D1CE4E5B9ULL; y ^= y >> 32; p[i].k[d] = (signed char)(((int)(y % (unsigned long long)W) - R.K/st)*st); }
+    }
+    std::vector<double> v; std::vector<unsigned char> nr;
+    long nq0 = R.nq; double u0 = R.u;
+    if(eval(R, p, NULL, v, nr)) return -1;
+    R.nq = nq0; R.u = u0;        /* the probe's fallback count and round column are its own; its
+                                    unresolved points are counted, as the global UNRESDROP does */
+    *zero = 1;
+    for(double x : v) if(x != 0){ *zero = 0; break; }
+    if(*zero) *nev += NP + 1;
+    return 0;
+}
+
+/* open-addressing set of nonzero 64-bit keys */
+struct KeySet {
+    std::vector<uint64_t> T; uint64_t mask = 0; long n = 0;
+    static uint64_t hh(uint64_t y){ return (y*0x9E3779B97F4A7C15ULL) >> 21; }
+    void init(long cap){ uint64_t c = 1 << 20; while(c < (uint64_t)cap*2) c <<= 1; T.assign(c, 0); mask = c - 1; n = 0; }
+    void grow(){ std::vector<uint64_t> O; O.swap(T); T.assign(O.size()*2, 0); mask = T.size() - 1; n = 0; for(uint64_t y : O) if(y) insert(y); }
+    /* 1 if y was new */
+    int insert(uint64_t y){
+        if((uint64_t)(n + 1)*10 > T.size()*7) grow();
+        uint64_t i = hh(y) & mask;
+        while(T[i]){ if(T[i] == y) return 0; i = (i + 1) & mask; }
+        T[i] = y; n++; return 1;
+    }
+    long find(uint64_t y) const { uint64_t i = hh(y) & mask; while(T[i]){ if(T[i] == y) return (long)i; i = (i + 1) & mask; } return -1; }
+};
+
+/* mixed-radix key (driver/sumkey.h:7-18): 1 c_0 ... c_{D-1} in base W, c_i = k_i/st + K/st; 0 if the
+ * keys would not fit 63 bits */
+static int keyradix(const Run &R, int st, uint64_t *P){
+    const uint64_t W = 2*(R.K/st) + 1, TOP = 1ULL << 63; uint64_t p = 1;
+    for(int i = R.D - 1; i >= 0; i--){ P[i] = p; if(p > TOP/W) return 0; p *= W; }
+    return (int)W;
+}
+static inline uint64_t key_of(const Run &R, const signed char *k, int st, int W){
+    uint64_t y = 1; for(int i = 0; i < R.D; i++) y = y*W + (uint64_t)(k[i]/st + R.K/st); return y;
+}
+static inline void key_pt(const Run &R, uint64_t y, int st, int W, sqb_pt_t *p){
+    memset(p, 0, sizeof *p);
+    for(int i = R.D - 1; i >= 0; i--){ p->k[i] = (signed char)(((int)(y % W) - R.K/st)*st); y /= W; }
+}
+
+struct GrowOut { double S, A, e1, e2, drop, gshs; long gshn, nev; };
+
+/* driver/sumkey.h:126-461 (see the file comment) */
+static int grow(Run &R, int lev, double eps_rel, std::vector<sqb_pt_t> &keep, GrowOut *go){
+    const int st = 1 << lev; uint64_t P[SQB_MAXD]; const int W = keyradix(R, st, P);
+    if(!W) FAIL("lattice too wide for 64-bit grid keys (D=%d, N=%d, step %dh)", R.D, 2*R.K + 1, st);
+    const double pw = pow(st, R.D);
+    const int store = lev > 0, gs = lev == 0 && R.o.abskip ? R.o.growskip : 0;
+    KeySet seen; seen.init(1 << 20);
+    std::vector<sqb_pt_t> fr(1), nx; memset(&fr[0], 0, sizeof fr[0]);
+    seen.insert(key_of(R, fr[0].k, st, W));
+    std::vector<double> kv, v; std::vector<unsigned char> nr, sk;
+    ksum ks; double a = 0, x1 = 0, x2 = 0, dr = 0, gshs = 0; long ne = 0, gshn = 0;
+    keep.clear();
+    while(!fr.empty()){
+        const long n = (long)fr.size();
+        sk.assign(n, 0);
+        if(gs) for(long i = 0; i < n; i++) sk[i] = fr[i].k[SQB_PFLAG] > 0;
+        if(eval(R, fr, gs ? sk.data() : NULL, v, nr)) return -1;
+        ne += n;
+        for(long i = 0; i < n; i++){ ks.add(v[i]*pw); a += fabs(v[i])*pw; }
+        const double thr = eps_rel*a;
+        std::vector<long> kj;
+        for(long i = 0; i < n; i++){
+            int mx = 0; for(int d = 0; d < R.D; d++){ int x = abs(fr[i].k[d]); if(x > mx) mx = x; }
+            const int kp = fabs(v[i]) >= thr;
+            const double w = fabs(v[i])*pw;
+            if(mx == R.K) x1 += w; else if(mx == R.K - st) x2 += w;
+            if(!kp){ dr += w; gshs += v[i]*pw; gshn++; }
+            else {
+                kj.push_back(i); kv.push_back(fabs(v[i]));
+                if(store){ sqb_pt_t p; memset(&p, 0, sizeof p); for(int d = 0; d < R.D; d++) p.k[d] = fr[i].k[d];
+                    if(R.o.abskip) p.k[SQB_PFLAG] = !nr[i];
+                    keep.push_back(p); }
+            }
+        }
+        /* the next frontier: unseen axis neighbours of the kept points, first occurrence wins */
+        nx.clear();
+        for(long j : kj){
+            const signed char *k = fr[j].k; const uint64_t y0 = key_of(R, k, st, W);
+            for(int d = 0; d < R.D; d++) for(int sg = -1; sg <= 1; sg += 2){
+                const int kk = k[d] + st*sg; if(kk > R.K || kk < -R.K) continue;
+                const uint64_t y = sg > 0 ? y0 + P[d] : y0 - P[d];
+                if(!seen.insert(y)) continue;
+                sqb_pt_t p; memcpy(&p, &fr[j], sizeof p); p.k[d] = (signed char)kk;
+                if(gs){ const int pg = fr[j].k[SQB_PFLAG]; p.k[SQB_PFLAG] = (signed char)(!sk[j] ? !nr[j] : (pg < gs ? pg + 1 : 0)); }
+                else p.k[SQB_PFLAG] = 0;
+                nx.push_back(p);
+            }
+        }
+        fr.swap(nx);
+    }
+    /* the final threshold, driver/sumkey.h:399-401 */
+    const double thr = eps_rel*a; long m = 0;
+    for(long i = 0; i < (long)kv.size(); i++){
+        if(kv[i] >= thr){ kv[m] = kv[i]; if(store) keep[m] = keep[i]; m++; } else dr += kv[i]*pw;
+    }
+    kv.resize(m); if(store) keep.resize(m);
+    /* shadow tiers by flood fill from z = 0, driver/sumkey.h:402-444 */
+    if(store && m && R.D < SQB_MAXD){
+        KeySet idx; idx.init(m); std::vector<long> hv(idx.T.size(), -1);
+        std::vector<uint64_t> KY(m);
+        for(long i = 0; i < m; i++){ KY[i] = key_of(R, keep[i].k, st, W); }
+        for(long i = 0; i < m; i++){ idx.insert(KY[i]); }
+        hv.assign(idx.T.size(), -1);
+        for(long i = 0; i < m; i++) hv[idx.find(KY[i])] = i;
+        std::vector<unsigned char> tr(m, 0); std::vector<long> cu, nw;
+        for(int t = 1; t <= 2; t++){
+            const double lim = (t == 1 ? 10 : 100)*thr;
+            cu.clear();
+            for(long i = 0; i < m; i++){ int z = 1; for(int d = 0; d < R.D; d++) if(keep[i].k[d]){ z = 0; break; }
+                if(z && kv[i] >= lim){ tr[i] = (unsigned char)t; cu.push_back(i); } }
+            while(!cu.empty()){
+                nw.clear();
+                for(long i : cu) for(int d = 0; d < R.D; d++) for(int sg = -1; sg <= 1; sg += 2){
+                    const int kk = keep[i].k[d] + st*sg; if(kk > R.K || kk < -R.K) continue;
+                    const uint64_t y = sg > 0 ? KY[i] + P[d] : KY[i] - P[d];
+                    const long q = idx.find(y); if(q < 0) continue;
+                    const long j = hv[q];
+                    if(kv[j] >= lim && tr[j] < t){ tr[j] = (unsigned char)t; nw.push_back(j); }
+                }
+                cu.swap(nw);
+            }
+        }
+        for(long i = 0; i < m; i++) keep[i].k[SQB_PFLAG] = (signed char)((keep[i].k[SQB_PFLAG] & 1) | (tr[i] << 1));
+    }
+    go->S = ks.val(); go->A = a; go->e1 = x1; go->e2 = x2; go->drop = dr; go->gshs = gshs; go->gshn = gshn; go->nev = ne;
+    return 0;
+}
+
+/* driver/sumkey.h:20-90: the cells and their axis neighbours at step st, merged flags, key order */
+static int dilate(Run &R, std::vector<sqb_pt_t> &cur, int st){
+    uint64_t P[SQB_MAXD]; const int W = keyradix(R, st, P);
+    if(!W) FAIL("lattice too wide for 64-bit grid keys in dilate");
+    const long n0 = (long)cur.size();
+    if(!n0) return 0;
+    std::vector<std::pair<uint64_t, unsigned char>> c; c.reserve(n0*(2*R.D + 1));
+    for(long q = 0; q < n0; q++){
+        const signed char *k = cur[q].k; const unsigned char fl = (unsigned char)k[SQB_PFLAG];
+        const uint64_t y0 = key_of(R, k, st, W);
+        c.push_back({y0, fl});
+        for(int j = 0; j < R.D; j++) for(int sg = -1; sg <= 1; sg += 2){
+            const int kk = k[j] + st*sg; if(kk > R.K || kk < -R.K) continue;
+            c.push_back({sg > 0 ? y0 + P[j] : y0 - P[j], fl});
+        }
+    }
+    std::sort(c.begin(), c.end(), [](const std::pair<uint64_t, unsigned char> &x, const std::pair<uint64_t, unsigned char> &y){ return x.first < y.first; });
+    cur.clear();
+    for(size_t i = 0; i < c.size();){
+        size_t j = i; int skb = 1, tr = 0;
+        while(j < c.size() && c[j].first == c[i].first){ skb &= c[j].second & 1; int t = c[j].second >> 1; if(t > tr) tr = t; j++; }
+        sqb_pt_t p; key_pt(R, c[i].first, st, W, &p); p.k[SQB_PFLAG] = (signed char)(skb | (tr << 1));
+        cur.push_back(p); i = j;
+    }
+    return 0;
+}
+
+static inline double ddv(const double *x){ return x[0] + x[1]; }
+
+extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top, const sqb_opts_t *opts, sqb_result_t *res){
+    memset(res, 0, sizeof *res);
+    Run R; R.g = sqb_find_graph(graph);
+    if(!R.g) FAIL("no graph %s in this build", graph);
+    if(opts) R.o = *opts; else sqb_default_opts(&R.o);
+    if(sqb_dev_init(R.o.device)) FAIL("device: %s", sqb_last_error());
+    if(top < 0){ top = 1; while(top < 2 && (1 << (top + 1))*h <= 3.0*(1 + 1e-9)) top++; }   /* driver/main.c:211-215 */
+    R.D = R.g->D; R.h = h; R.eps = eps; R.top = top;
+    if(R.D >= SQB_MAXD) FAIL("D=%d needs MAXD > 12", R.D);
+    const int m = 1 << (top + 1); int K = (N - 1)/2; K = ((K + m - 1)/m)*m;   /* driver/lattice.c:16 */
+    if(K > 127) FAIL("N = %d gives K = %d; points are stored in 8 bits, so K <= 127 (N <= 255)", N, K);
+    R.K = K;
+    R.X.resize(2*K + 1); R.Wt.resize(2*K + 1);
+    for(int k = -K; k <= K; k++){
+        if(R.g->zlattice){ R.X[k + K] = k*h; R.Wt[k + K] = h; }
+        else { R.X[k + K] = exp(k*h); R.Wt[k + K] = R.X[k + K]*h; }
+    }
+    if(sqb_dev_tables(R.X.data(), R.Wt.data(), K)) FAIL("device: %s", sqb_last_error());
+    const double t0 = now();
+    set_test(R, R.o.abserr0);
+    int zero = 0;
+    if(box_zero(R, top, &res->nev, &zero)) return -1;
+    if(zero){ res->zero = 1; res->t = now() - t0; return 0; }
+    std::vector<sqb_pt_t> cur; GrowOut go;
+    if(grow(R, top, eps*1e-3, cur, &go)) return -1;
+    res->nev += go.nev; res->ref = go.A; res->prune = go.drop;
+    if(top == 0 && go.gshn) res->prune = fabs(go.gshs);
+    if(go.A == 0){ res->t = now() - t0; res->nq = R.nq; return 0; }
+    { double r = go.e2 > 0 ? go.e1/go.e2 : 0; res->trunc = (r > 0 && r < 1) ? go.e1*r/(1 - r) : go.e1; }
+    for(int i = 0; i < 3; i++) res->S[i] = NAN;
+    double Slev[16]; int nl = 0; Slev[nl++] = go.S;
+    if(top > 0 && dilate(R, cur, 1 << top)) return -1;
+    res->kept_top = (long)cur.size();
+    res->t_top = now() - t0;
+    const int esok = R.D < SQB_MAXD && top > 0;
+    /* the levels on the device */
+    set_test(R, fmax(R.o.abserr0, R.o.abrel*eps*res->ref));    /* driver/sum.c:651 */
+    sqb_pt_t *dcur = NULL, *dnext = NULL; long ncur = (long)cur.size(), next_cap = 0;
+    if(top > 0){
+        dcur = (sqb_pt_t*)sqb_dev_alloc(ncur*sizeof(sqb_pt_t));
+        if(!dcur) FAIL("device allocation of %ld cells failed", ncur);
+        if(sqb_dev_upload(dcur, cur.data(), ncur*sizeof(sqb_pt_t))){ sqb_dev_free(dcur); FAIL("device: %s", sqb_last_error()); }
+    }
+    std::vector<sqb_pt_t>().swap(cur);
+    const double tl0 = now(); double es1 = 0, es2 = 0, ah = 0, uu = 0;
+    for(int lev = top - 1; lev >= 0; lev--){
+        const int st = 1 << lev, last = lev == 0;
+        sqb_level_t L; memset(&L, 0, sizeof L);
+        L.g = R.g; L.cells = dcur; L.ncell = ncur; L.st = st; L.last = last;
+        L.pw = pow(st, R.D); L.thr = eps*res->ref*1e-2; L.t = R.t; L.max_children = R.o.max_children;
+        if(!last){
+            double want = (double)ncur*(double)(1L << R.D);
+            double room = 0.45*(double)sqb_dev_free_bytes()/sizeof(sqb_pt_t);
+            next_cap = (long)(want < room ? want : room) + 1;
+            dnext = (sqb_pt_t*)sqb_dev_alloc(next_cap*sizeof(sqb_pt_t));
+            if(!dnext){ sqb_dev_free(dcur); FAIL("device allocation of the next level (%ld cells) failed", next_cap); }
+            L.next = dnext; L.next_cap = next_cap;
+        }
+        sqb_acc_t acc; memset(&acc, 0, sizeof acc); long nn = 0; double ms = 0;
+        if(sqb_dev_level(&L, &acc, &nn, &ms)){ sqb_dev_free(dcur); sqb_dev_free(dnext); FAIL("device: %s", sqb_last_error()); }
+        if(acc.overflow){ sqb_dev_free(dcur); sqb_dev_free(dnext); FAIL("level %d: %ld kept cells exceed the device list (%ld)", lev, nn, next_cap); }
+        Slev[nl++] = ddv(acc.S);
+        res->prune += ddv(acc.drop); res->nev += (long)acc.ne; R.nq += (long)acc.nq; R.unresdrop += (long)acc.unres;
+        res->abskipped += (long)acc.skipped;
+        if(res->nlev < 16){ res->lev_evals[res->nlev] = (long)acc.ne; res->lev_ms[res->nlev] = ms; res->nlev++; }
+        if(last){ ah = ddv(acc.A); uu = ddv(acc.u); es1 = ddv(acc.b1); es2 = ddv(acc.b2); }
+        if(R.o.verbose) fprintf(stderr, "# %s level step %dh: %ld cells, %llu evals, %llu fallback, %ld kept, %.1f ms\n",
+                                R.g->name, st, ncur, acc.ne, acc.nq, nn, ms);
+        sqb_dev_free(dcur); dcur = dnext; dnext = NULL; ncur = last ? 0 : nn;
+    }
+    sqb_dev_free(dcur);
+    res->t_levels = now() - tl0;
+    if(top > 0){ res->unres = sqrt(uu); res->Ah = ah; }
+    else res->unres = sqrt(R.u);
+    res->S[0] = Slev[nl - 1]; res->S[1] = nl > 1 ? Slev[nl - 2] : NAN; res->S[2] = nl > 2 ? Slev[nl - 3] : NAN;
+    res->es1 = es1; res->es2 = es2; res->esok = esok;
+    res->nq = R.nq; res->unresdrop = R.unresdrop;
+    res->t = now() - t0;
+    return 0;
+}
+
+/* pointwise kernel evaluation for parity checks */
+extern "C" int sqb_eval_points_impl(const sqb_graph_t *g, long n, const double *sf, int prec, int ab, double *f, double *abs_);
+extern "C" int sqb_eval_points(const char *graph, long n, const double *sf, int prec, int ab, double *f, double *abs_){
+    const sqb_graph_t *g = sqb_find_graph(graph);
+    if(!g) FAIL("no graph %s in this build", graph);
+    if(sqb_dev_init(0)) FAIL("device: %s", sqb_last_error());
+    if(sqb_eval_points_impl(g, n, sf, prec, ab, f, abs_)) FAIL("device: %s", sqb_last_error());
+    return 0;
+}

@@ -1,0 +1,529 @@
+/* runtime.cu -- the device layer: device state, node-batch evaluation with the precision fallback, the
+ * device-resident refinement level (evaluate, fall back, reduce, keep), and the reference's GPU plug-in
+ * ABI (the plain form, driver/gpu.h:12-22).
+ *
+ * A refinement level (driver/sum.c:652-799) is run on the device in batches of cells:
+ *   1. sqb_k_f64 (per graph): every child in FP64 with the per-point tests; points whose |.| bound is
+ *      above ABSERR are queued;
+ *   2. sqb_k_dd (per graph): the queued points in double-double (qvalue semantics);
+ *   3. sqb_k_reduce: per tile of children (in cell order, b ascending), compensated double-double sums of
+ *      v*pw, |v|, the dropped weight, the shadow-tier sums and the round column, plus counters and the
+ *      number of kept children;
+ *   4. sqb_k_finish (one CTA): exclusive scan of the tiles' kept counts and the tiles' sums added in
+ *      a fixed order into the level accumulator, so that a run is reproducible;
+ *   5. sqb_k_scatter: the kept children written, in order, to the next level's cell list with their
+ *      flags (skip bit, shadow tier; driver/sum.c:741-745).
+ * Nothing goes back to the host until the level ends: the host reads the accumulator once per level. */
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include <omp.h>
+#include "sqb_rt.h"
+#include "sqdd.cuh"
+#include "sincfeyn_b200.h"
+
+extern "C" const sqb_graph_t *const SQB_ALL[];
+extern "C" const int SQB_NALL;
+
+static char g_err[512];
+#define CKR(x) do { cudaError_t e_ = (x); if(e_ != cudaSuccess){                                    \
+    snprintf(g_err, sizeof g_err, "%s at %s:%d: %s", #x, __FILE__, __LINE__, cudaGetErrorString(e_)); \
+    return (int)e_; } } while(0)
+
+extern "C" const char *sqb_last_error(void){ return g_err; }
+
+extern "C" const sqb_graph_t *sqb_find_graph(const char *name){
+    for(int i = 0; i < SQB_NALL; i++) if(!strcmp(SQB_ALL[i]->name, name) || !strcmp(SQB_ALL[i]->volkov, name)) return SQB_ALL[i];
+    return NULL;
+}
+extern "C" int sqb_ngraphs(void){ return SQB_NALL; }
+extern "C" const sqb_graph_t *sqb_graph_at(int i){ return i >= 0 && i < SQB_NALL ? SQB_ALL[i] : NULL; }
+
+/* ------------------------------------------------------------------------------------------------ */
+#define RT 256                    /* threads per reduce / scatter CTA */
+#define RPT 8                     /* consecutive children per thread */
+#define RTILE (RT*RPT)
+#define FT 256                    /* threads of the one-CTA finish kernel */
+
+typedef struct {
+    double S[2], A[2], drop[2], b1[2], b2[2], u[2];
+    unsigned long long ne, nq, unres, skipped;
+} part_t;
+
+typedef struct {
+    const signed char *cells;     /* device pt_t list (12 bytes per cell) */
+    long n;                       /* children in this batch */
+    int D, st, last, abskip;
+    double pw, thr;
+    const double *v, *uu;
+    const unsigned char *stt;
+} lvl_t;
+
+struct Dev {
+    int on, dev, nsm;
+    char info[256];
+    cudaStream_t s;
+    cudaEvent_t e0, e1;
+    double *X, *Wt; int tabcap, K;
+    long cap;                      /* points per batch */
+    double *v, *uu; unsigned char *stt; long *fb; unsigned long long *nfb;
+    long nbcap; part_t *bp; unsigned *bkeep; unsigned long long *boff;
+    sqb_acc_t *acc; unsigned long long *base;
+    long dcap; sqb_pt_t *dpts; unsigned char *dskip;
+    long hcap; sqb_pt_t *hpts; unsigned char *hskip, *hst; double *hv, *huu;
+};
+static Dev G;
+
+extern "C" int sqb_dev_init(int device){
+    if(G.on) return 0;
+    int nd = 0; CKR(cudaGetDeviceCount(&nd));
+    if(nd == 0){ snprintf(g_err, sizeof g_err, "no CUDA device"); return -1; }
+    if(device < 0 || device >= nd) device = 0;
+    CKR(cudaSetDevice(device));
+    cudaDeviceProp p; CKR(cudaGetDeviceProperties(&p, device));
+    G.dev = device; G.nsm = p.multiProcessorCount;
+    snprintf(G.info, sizeof G.info, "%s (sm_%d%d, %d SMs)", p.name, p.major, p.minor, p.multiProcessorCount);
+    CKR(cudaStreamCreateWithFlags(&G.s, cudaStreamNonBlocking));
+    CKR(cudaEventCreate(&G.e0)); CKR(cudaEventCreate(&G.e1));
+    CKR(cudaMalloc(&G.acc, sizeof(sqb_acc_t)));
+    CKR(cudaMalloc(&G.base, sizeof(unsigned long long)));
+    CKR(cudaMalloc(&G.nfb, sizeof(unsigned long long)));
+    G.on = 1;
+    return 0;
+}
+extern "C" const char *sqb_dev_info(void){ return G.on ? G.info : "off"; }
+
+extern "C" int sqb_dev_tables(const double *X, const double *Wt, int K){
+    int nt = 2*K + 1;
+    if(nt > G.tabcap){
+        if(G.X){ cudaFree(G.X); cudaFree(G.Wt); }
+        CKR(cudaMalloc(&G.X, nt*sizeof(double))); CKR(cudaMalloc(&G.Wt, nt*sizeof(double)));
+        G.tabcap = nt;
+    }
+    CKR(cudaMemcpy(G.X, X, nt*sizeof(double), cudaMemcpyHostToDevice));
+    CKR(cudaMemcpy(G.Wt, Wt, nt*sizeof(double), cudaMemcpyHostToDevice));
+    G.K = K;
+    return 0;
+}
+
+static int reserve_points(long n){
+    if(n <= G.cap) return 0;
+    long c = 1L << 16; while(c < n) c <<= 1;
+    if(G.v){ cudaFree(G.v); cudaFree(G.uu); cudaFree(G.stt); cudaFree(G.fb); cudaFree(G.bp); cudaFree(G.bkeep); cudaFree(G.boff); }
+    CKR(cudaMalloc(&G.v, c*sizeof(double))); CKR(cudaMalloc(&G.uu, c*sizeof(double)));
+    CKR(cudaMalloc(&G.stt, c)); CKR(cudaMalloc(&G.fb, c*sizeof(long)));
+    long nb = (c + RTILE - 1)/RTILE;
+    CKR(cudaMalloc(&G.bp, nb*sizeof(part_t))); CKR(cudaMalloc(&G.bkeep, nb*sizeof(unsigned)));
+    CKR(cudaMalloc(&G.boff, nb*sizeof(unsigned long long)));
+    G.cap = c; G.nbcap = nb;
+    return 0;
+}
+
+static int grid_for(const sqb_graph_t *g, int which, long npts, size_t smem){
+    sqb_kattr_t at; int per = 2;
+    if(g->attr(which, 128, smem, &at) && at.blocks_per_sm > 0) per = at.blocks_per_sm;
+    long want = (npts + 127)/128, full = (long)G.nsm*per;
+    if(want < 1) want = 1;
+    return (int)(want < full ? want : full);
+}
+
+static void fill_eval(sqb_eval_t *a, const sqb_test_t *t){
+    a->X = G.X; a->Wt = G.Wt; a->K = G.K; a->H = 0; a->raw = 0;
+    a->abskip = t->abskip; a->abcheck = t->abcheck;
+    a->abserr = t->abserr; a->near_thr = t->nearf*t->abserr; a->ddslack = t->ddslack;
+    a->v = G.v; a->ab = NULL; a->stt = G.stt; a->fb = G.fb; a->nfb = G.nfb; a->fbcap = G.cap;
+}
+
+/* FP64 pass (or the all-dd pass) and the fallback pass for one batch already described by a */
+static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, long npts){
+    size_t smem = 2*(2*G.K + 1)*sizeof(double);
+    sqb_dd_t d; memset(&d, 0, sizeof d);
+    d.e = *a; d.dropunres = t->dropunres; d.uu = G.uu;
+    if(t->alldd){
+        d.all = 1;
+        g->dd(&d, grid_for(g, 1, npts, smem), 128, smem, G.s);
+        CKR(cudaGetLastError());
+        return 0;
+    }
+    CKR(cudaMemsetAsync(G.nfb, 0, sizeof(unsigned long long), G.s));
+    g->f64(a, grid_for(g, 0, npts, smem), 128, smem, G.s);
+    CKR(cudaGetLastError());
+    d.list = G.fb; d.nlist = G.nfb; d.listcap = G.cap; d.all = 0;
+    /* the queue length is known only on the device: a persistent grid reads it */
+    g->dd(&d, grid_for(g, 1, 1L << 30, smem), 128, smem, G.s);
+    CKR(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int sqb_dev_eval_nodes(const sqb_graph_t *g, long n, const sqb_pt_t *pts, const unsigned char *skip,
+                                  const sqb_test_t *t, double *v, unsigned char *near, long *nq, double *u, long *unres){
+    if(n <= 0) return 0;
+    const long CH = 1L << 22;
+    long m0 = n < CH ? n : CH;
+    if(reserve_points(m0)) return -1;
+    if(m0 > G.dcap){
+        if(G.dpts){ cudaFree(G.dpts); cudaFree(G.dskip); cudaFreeHost(G.hpts); cudaFreeHost(G.hskip); cudaFreeHost(G.hv); cudaFreeHost(G.hst); cudaFreeHost(G.huu); }
+        long c = 1L << 16; while(c < m0) c <<= 1;
+        CKR(cudaMalloc(&G.dpts, c*sizeof(sqb_pt_t))); CKR(cudaMalloc(&G.dskip, c));
+        CKR(cudaMallocHost(&G.hpts, c*sizeof(sqb_pt_t))); CKR(cudaMallocHost(&G.hskip, c));
+        CKR(cudaMallocHost(&G.hv, c*sizeof(double))); CKR(cudaMallocHost(&G.hst, c)); CKR(cudaMallocHost(&G.huu, c*sizeof(double)));
+        G.dcap = c; G.hcap = c;
+    }
+    long q = 0, nd = 0; double uu = 0;
+    for(long i0 = 0; i0 < n; i0 += CH){
+        long m = n - i0 < CH ? n - i0 : CH;
+        memcpy(G.hpts, pts + i0, m*sizeof(sqb_pt_t));
+        CKR(cudaMemcpyAsync(G.dpts, G.hpts, m*sizeof(sqb_pt_t), cudaMemcpyHostToDevice, G.s));
+        if(skip){ memcpy(G.hskip, skip + i0, m); CKR(cudaMemcpyAsync(G.dskip, G.hskip, m, cudaMemcpyHostToDevice, G.s)); }
+        sqb_eval_t a; memset(&a, 0, sizeof a); fill_eval(&a, t);
+        a.pts = G.dpts; a.n = m; a.esize = 1; a.stride = SQB_MAXD; a.flag_at = -1; a.cells = 0; a.st = 0;
+        a.skip = skip ? G.dskip : NULL;
+        if(eval_batch(g, &a, t, m)) return -1;
+        CKR(cudaMemcpyAsync(G.hv, G.v, m*sizeof(double), cudaMemcpyDeviceToHost, G.s));
+        CKR(cudaMemcpyAsync(G.hst, G.stt, m, cudaMemcpyDeviceToHost, G.s));
+        CKR(cudaMemcpyAsync(G.huu, G.uu, m*sizeof(double), cudaMemcpyDeviceToHost, G.s));
+        CKR(cudaStreamSynchronize(G.s));
+        for(long i = 0; i < m; i++){
+            unsigned char s = G.hst[i];
+            v[i0 + i] = G.hv[i];
+            if(near) near[i0 + i] = (s & SQB_NEAR) ? 1 : 0;
+            if(s & SQB_FALLBACK){ q++; uu += G.huu[i]; }
+            if(s & SQB_UNRES) nd++;
+        }
+    }
+    *nq += q; *u += uu; *unres += nd;
+    return 0;
+}
+
+/* ---------------------------------------- level reduce ------------------------------------------ */
+__device__ __forceinline__ sqdd shfl_dd(const sqdd &a, int off){
+    return sqdd(__shfl_down_sync(0xffffffffu, a.hi, off), __shfl_down_sync(0xffffffffu, a.lo, off));
+}
+__device__ __forceinline__ int parent_tier(const lvl_t &a, long i){
+    const long c = i >> a.D;
+    return (a.cells[c*SQB_MAXD + SQB_PFLAG] >> 1) & 3;
+}
+
+__global__ void __launch_bounds__(RT) sqb_k_reduce(const lvl_t a, part_t *bp, unsigned *bkeep){
+    const long t0 = blockIdx.x*(long)RTILE + threadIdx.x*(long)RPT;
+    sqdd S, A, dr, b1, b2, u;
+    unsigned ne = 0, nq = 0, nu = 0, nsk = 0, keep = 0;
+    for(int j = 0; j < RPT; j++){
+        const long i = t0 + j;
+        if(i >= a.n) break;
+        const unsigned char s = a.stt[i];
+        if(!(s & SQB_PRESENT)) continue;
+        const double v = a.v[i], vp = v*a.pw, av = fabs(v);
+        S = sqdd_add_d(S, vp); A = sqdd_add_d(A, av); ne++;
+        nsk += (s & SQB_SKIPPED) ? 1 : 0;
+        if(s & SQB_FALLBACK){ nq++; u = sqdd_add_d(u, a.uu[i]); }
+        if(s & SQB_UNRES) nu++;
+        if(a.last){
+            const int te = parent_tier(a, i);
+            if(te >= 1) b1 = sqdd_add_d(b1, vp);
+            if(te >= 2) b2 = sqdd_add_d(b2, vp);
+        } else if(av >= a.thr) keep++;
+        else dr = sqdd_add_d(dr, av*a.pw);
+    }
+    for(int off = 16; off; off >>= 1){
+        S = S + shfl_dd(S, off); A = A + shfl_dd(A, off); dr = dr + shfl_dd(dr, off);
+        b1 = b1 + shfl_dd(b1, off); b2 = b2 + shfl_dd(b2, off); u = u + shfl_dd(u, off);
+        ne += __shfl_down_sync(0xffffffffu, ne, off); nq += __shfl_down_sync(0xffffffffu, nq, off);
+        nu += __shfl_down_sync(0xffffffffu, nu, off); nsk += __shfl_down_sync(0xffffffffu, nsk, off);
+        keep += __shfl_down_sync(0xffffffffu, keep, off);
+    }
+    __shared__ part_t wp[RT/32];
+    __shared__ unsigned wk[RT/32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if(l == 0){
+        part_t p; p.S[0] = S.hi; p.S[1] = S.lo; p.A[0] = A.hi; p.A[1] = A.lo; p.drop[0] = dr.hi; p.drop[1] = dr.lo;
+        p.b1[0] = b1.hi; p.b1[1] = b1.lo; p.b2[0] = b2.hi; p.b2[1] = b2.lo; p.u[0] = u.hi; p.u[1] = u.lo;
+        p.ne = ne; p.nq = nq; p.unres = nu; p.skipped = nsk;
+        wp[w] = p; wk[w] = keep;
+    }
+    __syncthreads();
+    if(threadIdx.x == 0){
+        part_t r = wp[0]; unsigned k = wk[0];
+        for(int j = 1; j < RT/32; j++){
+            const part_t &p = wp[j];
+#define ADDP(F) { sqdd x = sqdd(r.F[0], r.F[1]) + sqdd(p.F[0], p.F[1]); r.F[0] = x.hi; r.F[1] = x.lo; }
+            ADDP(S) ADDP(A) ADDP(drop) ADDP(b1) ADDP(b2) ADDP(u)
+            r.ne += p.ne; r.nq += p.nq; r.unres += p.unres; r.skipped += p.skipped; k += wk[j];
+        }
+        bp[blockIdx.x] = r; bkeep[blockIdx.x] = k;
+    }
+}
+
+/* one CTA: the tiles' offsets (exclusive scan of their kept counts) and the batch's sums, in a fixed
+ * order, added into the level accumulator; *base = this batch's first slot in the next list */
+__global__ void __launch_bounds__(FT) sqb_k_finish(const part_t *bp, const unsigned *bkeep, long nb,
+                                                   unsigned long long *boff, sqb_acc_t *acc, unsigned long long *base){
+    __shared__ double sh[FT][12];
+    __shared__ unsigned long long sc[FT][5];
+    const int t = threadIdx.x;
+    const long ch = (nb + FT - 1)/FT, j0 = t*ch, j1 = j0 + ch < nb ? j0 + ch : nb;
+    sqdd S, A, dr, b1, b2, u; unsigned long long ne = 0, nq = 0, nu = 0, nsk = 0, kp = 0;
+    for(long j = j0; j < j1; j++){
+        const part_t &p = bp[j];
+        S = S + sqdd(p.S[0], p.S[1]); A = A + sqdd(p.A[0], p.A[1]); dr = dr + sqdd(p.drop[0], p.drop[1]);
+        b1 = b1 + sqdd(p.b1[0], p.b1[1]); b2 = b2 + sqdd(p.b2[0], p.b2[1]); u = u + sqdd(p.u[0], p.u[1]);
+        ne += p.ne; nq += p.nq; nu += p.unres; nsk += p.skipped; kp += bkeep[j];
+    }
+    sh[t][0] = S.hi; sh[t][1] = S.lo; sh[t][2] = A.hi; sh[t][3] = A.lo; sh[t][4] = dr.hi; sh[t][5] = dr.lo;
+    sh[t][6] = b1.hi; sh[t][7] = b1.lo; sh[t][8] = b2.hi; sh[t][9] = b2.lo; sh[t][10] = u.hi; sh[t][11] = u.lo;
+    sc[t][0] = ne; sc[t][1] = nq; sc[t][2] = nu; sc[t][3] = nsk; sc[t][4] = kp;
+    __syncthreads();
+    /* exclusive scan of the per-thread kept counts (thread 0, FT values), then per-tile offsets */
+    __shared__ unsigned long long pre[FT];
+    if(t == 0){ unsigned long long x = 0; for(int j = 0; j < FT; j++){ pre[j] = x; x += sc[j][4]; } }
+    __syncthreads();
+    { unsigned long long x = pre[t]; for(long j = j0; j < j1; j++){ boff[j] = x; x += bkeep[j]; } }
+    /* fixed-order tree of the sums */
+    for(int h = FT/2; h; h >>= 1){
+        if(t < h){
+            for(int q = 0; q < 12; q += 2){
+                sqdd x = sqdd(sh[t][q], sh[t][q + 1]) + sqdd(sh[t + h][q], sh[t + h][q + 1]);
+                sh[t][q] = x.hi; sh[t][q + 1] = x.lo;
+            }
+            for(int q = 0; q < 4; q++) sc[t][q] += sc[t + h][q];
+        }
+        __syncthreads();
+    }
+    if(t == 0){
+        unsigned long long total = pre[FT - 1] + sc[FT - 1][4];
+        double *dst[6] = {acc->S, acc->A, acc->drop, acc->b1, acc->b2, acc->u};
+        for(int q = 0; q < 6; q++){
+            sqdd x = sqdd(dst[q][0], dst[q][1]) + sqdd(sh[0][2*q], sh[0][2*q + 1]);
+            dst[q][0] = x.hi; dst[q][1] = x.lo;
+        }
+        acc->ne += sc[0][0]; acc->nq += sc[0][1]; acc->unres += sc[0][2]; acc->skipped += sc[0][3];
+        *base = acc->keep; acc->keep += total;
+    }
+}
+
+__global__ void __launch_bounds__(RT) sqb_k_scatter(const lvl_t a, const unsigned long long *boff,
+                                                    const unsigned long long *base, sqb_pt_t *next, long cap,
+                                                    unsigned long long *overflow){
+    const long t0 = blockIdx.x*(long)RTILE + threadIdx.x*(long)RPT;
+    unsigned mask = 0; int cnt = 0;
+    for(int j = 0; j < RPT; j++){
+        const long i = t0 + j;
+        if(i >= a.n) break;
+        if((a.stt[i] & SQB_PRESENT) && fabs(a.v[i]) >= a.thr){ mask |= 1u << j; cnt++; }
+    }
+    /* block exclusive scan of cnt */
+    __shared__ int ws[RT/32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    int x = cnt;
+    for(int off = 1; off < 32; off <<= 1){ int y = __shfl_up_sync(0xffffffffu, x, off); if(l >= off) x += y; }
+    if(l == 31) ws[w] = x;
+    __syncthreads();
+    if(threadIdx.x == 0){ int s = 0; for(int j = 0; j < RT/32; j++){ int y = ws[j]; ws[j] = s; s += y; } }
+    __syncthreads();
+    unsigned long long o = *base + boff[blockIdx.x] + (unsigned long long)(ws[w] + x - cnt);
+    const double thr10 = 10*a.thr, thr100 = 100*a.thr;
+    for(int j = 0; j < RPT; j++){
+        if(!(mask >> j & 1)) continue;
+        const long i = t0 + j;
+        if((long)o >= cap){ atomicAdd(overflow, 1ULL); o++; continue; }
+        const long c = i >> a.D; const int b = (int)(i & ((1L << a.D) - 1));
+        const signed char *p = a.cells + c*SQB_MAXD;
+        const unsigned char s = a.stt[i];
+        const double av = fabs(a.v[i]);
+        const int te = (p[SQB_PFLAG] >> 1) & 3, tv = (av >= thr10) + (av >= thr100);
+        const int psk = (s & SQB_SKIPPED) ? 1 : 0, nr = (s & SQB_NEAR) ? 1 : 0;
+        union { signed char k[SQB_MAXD]; int w[3]; } q;
+        q.w[0] = q.w[1] = q.w[2] = 0;
+        for(int d = 0; d < a.D; d++) q.k[d] = (signed char)(p[d] - (((b >> d) & 1) ? a.st : 0));
+        q.k[SQB_PFLAG] = (signed char)((a.abskip && (psk || !nr)) | ((te < tv ? te : tv) << 1));
+        int *dst = (int*)(next + o);
+        dst[0] = q.w[0]; dst[1] = q.w[1]; dst[2] = q.w[2];
+        o++;
+    }
+}
+
+extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n, double *ms){
+    const sqb_graph_t *g = L->g; const int D = g->D;
+    long maxch = L->max_children > 0 ? L->max_children : (1L << 25);
+    if(maxch < (1L << D)) maxch = 1L << D;
+    long ncb = maxch >> D;
+    if(reserve_points(ncb << D)) return -1;
+    CKR(cudaMemsetAsync(G.acc, 0, sizeof(sqb_acc_t), G.s));
+    CKR(cudaEventRecord(G.e0, G.s));
+    for(long c0 = 0; c0 < L->ncell; c0 += ncb){
+        const long nc = L->ncell - c0 < ncb ? L->ncell - c0 : ncb, nch = nc << D;
+        const sqb_pt_t *cells = L->cells + c0;
+        sqb_eval_t a; memset(&a, 0, sizeof a); fill_eval(&a, &L->t);
+        a.pts = cells; a.n = nc; a.esize = 1; a.stride = SQB_MAXD; a.flag_at = SQB_PFLAG; a.cells = 1; a.st = L->st;
+        if(eval_batch(g, &a, &L->t, nch)) return -1;
+        lvl_t r; r.cells = (const signed char*)cells; r.n = nch; r.D = D; r.st = L->st; r.last = L->last;
+        r.abskip = L->t.abskip; r.pw = L->pw; r.thr = L->thr; r.v = G.v; r.uu = G.uu; r.stt = G.stt;
+        const long nb = (nch + RTILE - 1)/RTILE;
+        sqb_k_reduce<<<(unsigned)nb, RT, 0, G.s>>>(r, G.bp, G.bkeep);
+        CKR(cudaGetLastError());
+        sqb_k_finish<<<1, FT, 0, G.s>>>(G.bp, G.bkeep, nb, G.boff, G.acc, G.base);
+        CKR(cudaGetLastError());
+        if(!L->last){
+            sqb_k_scatter<<<(unsigned)nb, RT, 0, G.s>>>(r, G.boff, G.base, L->next, L->next_cap, &G.acc->overflow);
+            CKR(cudaGetLastError());
+        }
+    }
+    CKR(cudaEventRecord(G.e1, G.s));
+    sqb_acc_t h;
+    CKR(cudaMemcpyAsync(&h, G.acc, sizeof h, cudaMemcpyDeviceToHost, G.s));
+    CKR(cudaStreamSynchronize(G.s));
+    float t = 0; cudaEventElapsedTime(&t, G.e0, G.e1); if(ms) *ms = t;
+    double *src[6] = {h.S, h.A, h.drop, h.b1, h.b2, h.u}, *dst[6] = {acc->S, acc->A, acc->drop, acc->b1, acc->b2, acc->u};
+    for(int q = 0; q < 6; q++){ sqdd x = sqdd(dst[q][0], dst[q][1]) + sqdd(src[q][0], src[q][1]); dst[q][0] = x.hi; dst[q][1] = x.lo; }
+    acc->ne += h.ne; acc->nq += h.nq; acc->unres += h.unres; acc->skipped += h.skipped; acc->keep += h.keep; acc->overflow += h.overflow;
+    *next_n = (long)h.keep;
+    return 0;
+}
+
+extern "C" void *sqb_dev_alloc(size_t bytes){ void *p = NULL; if(cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess){ cudaGetLastError(); return NULL; } return p; }
+extern "C" void sqb_dev_free(void *p){ if(p) cudaFree(p); }
+extern "C" int sqb_dev_upload(void *dst, const void *src, size_t bytes){ CKR(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice)); return 0; }
+extern "C" int sqb_dev_download(void *dst, const void *src, size_t bytes){ CKR(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost)); return 0; }
+extern "C" size_t sqb_dev_free_bytes(void){ size_t f = 0, t = 0; cudaMemGetInfo(&f, &t); return f; }
+
+/* ------------------------------ plain form: the reference's GPU plug-in ABI ---------------------- */
+/* Same contract as driver/gpu.cu:1-103: two slots, each with its own stream, event and pinned buffers;
+ * gpu_submit* pack the coordinates (here to int8: |k| <= 127, driver/sq.h:117), copy, launch and copy
+ * back f*w and |.|*w; gpu_wait waits for the slot.  SINCQED_GPU=0 turns the GPU off, SINCQED_GPU=d
+ * picks device d-1.  CUDA errors print and exit(3), as the reference does. */
+#define CKX(x) do { cudaError_t e_ = (x); if(e_ != cudaSuccess){ fprintf(stderr, "CUDA error %s at %s:%d: %s\n", #x, __FILE__, __LINE__, cudaGetErrorString(e_)); exit(3); } } while(0)
+
+typedef struct { cudaStream_t st; cudaEvent_t ev; long cap, n; signed char *hK, *dK; unsigned char *hS, *dS; double *hF, *hA, *dF, *dA; } pslot_t;
+static pslot_t PS[2];
+static int PON = -1, PD, PK; static double PH;
+static const sqb_graph_t *PCUR;
+static double *PEX; static int PEXN;
+
+static int plain_init(void){
+    if(PON >= 0) return PON;
+    const char *e = getenv("SINCQED_GPU"); PON = 0;
+    if(e && !strcmp(e, "0")) return 0;
+    int nd = 0; if(cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0){ cudaGetLastError(); return 0; }
+    int dev = e && atoi(e) > 0 ? atoi(e) - 1 : 0; if(dev >= nd) dev = 0;
+    if(sqb_dev_init(dev)){ fprintf(stderr, "gpu: %s\n", g_err); exit(3); }
+    for(int b = 0; b < 2; b++){ CKX(cudaStreamCreateWithFlags(&PS[b].st, cudaStreamNonBlocking)); CKX(cudaEventCreateWithFlags(&PS[b].ev, cudaEventDisableTiming)); }
+    return PON = 1;
+}
+static void plain_reserve(pslot_t *s, long n){
+    if(n <= s->cap) return;
+    if(s->cap){ cudaFreeHost(s->hK); cudaFree(s->dK); cudaFreeHost(s->hS); cudaFree(s->dS); cudaFreeHost(s->hF); cudaFree(s->dF); cudaFreeHost(s->hA); cudaFree(s->dA); }
+    long c = 1L << 16; while(c < n) c <<= 1; s->cap = c;
+    CKX(cudaMallocHost(&s->hK, c*SQB_MAXD)); CKX(cudaMalloc(&s->dK, c*SQB_MAXD));
+    CKX(cudaMallocHost(&s->hS, c)); CKX(cudaMalloc(&s->dS, c));
+    CKX(cudaMallocHost(&s->hF, c*sizeof(double))); CKX(cudaMalloc(&s->dF, c*sizeof(double)));
+    CKX(cudaMallocHost(&s->hA, c*sizeof(double))); CKX(cudaMalloc(&s->dA, c*sizeof(double)));
+}
+
+extern "C" const char *gpu_info(void){ return PON == 1 ? G.info : "off"; }
+
+extern "C" int gpu_setup(const char *name, int D, const double *EX, int K, double H){
+    PCUR = NULL;
+    if(!plain_init()) return 0;
+    const sqb_graph_t *g = sqb_find_graph(name);
+    if(!g || strcmp(g->name, name)) return 0;
+    if(g->D != D){ fprintf(stderr, "gpu: %s has D=%d, expected %d\n", name, g->D, D); exit(3); }
+    PCUR = g; PD = D; PK = K; PH = H;
+    CKX(cudaDeviceSynchronize());
+    if(PEXN < 2*K + 1){ if(PEX) CKX(cudaFree(PEX)); PEXN = 2*K + 1; CKX(cudaMalloc(&PEX, PEXN*sizeof(double))); }
+    CKX(cudaMemcpy(PEX, EX, (2*K + 1)*sizeof(double), cudaMemcpyHostToDevice));
+    return 1;
+}
+
+static void plain_launch(pslot_t *s, long npts, long nrows, int cells, int st, int has_skip){
+    sqb_eval_t a; memset(&a, 0, sizeof a);
+    a.pts = s->dK; a.n = nrows; a.esize = 1; a.stride = PD; a.flag_at = -1; a.cells = cells; a.st = st;
+    a.X = PEX; a.Wt = NULL; a.K = PK; a.H = PH; a.raw = 1; a.skip = has_skip ? s->dS : NULL;
+    a.v = s->dF; a.ab = s->dA;
+    size_t smem = 2*(2*PK + 1)*sizeof(double);
+    PCUR->f64(&a, grid_for(PCUR, 0, npts, smem), 128, smem, s->st);
+    CKX(cudaGetLastError());
+}
+
+extern "C" void gpu_submit(int slot, long n, const int *k, int stride, const unsigned char *skip){
+    pslot_t *s = &PS[slot]; plain_reserve(s, n); s->n = n;
+    if(n <= 0) return;
+    signed char *hk = s->hK; const int D = PD;
+    #pragma omp parallel for schedule(static)
+    for(long i = 0; i < n; i++) for(int d = 0; d < D; d++) hk[i*D + d] = (signed char)k[i*stride + d];
+    CKX(cudaMemcpyAsync(s->dK, hk, n*D, cudaMemcpyHostToDevice, s->st));
+    if(skip){ memcpy(s->hS, skip, n); CKX(cudaMemcpyAsync(s->dS, s->hS, n, cudaMemcpyHostToDevice, s->st)); }
+    plain_launch(s, n, n, 0, 0, skip != NULL);
+    CKX(cudaMemcpyAsync(s->hF, s->dF, n*sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CKX(cudaMemcpyAsync(s->hA, s->dA, n*sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CKX(cudaEventRecord(s->ev, s->st));
+}
+
+extern "C" void gpu_submit_cells(int slot, long nc, const int *cells, int stride, const unsigned char *skip, int st){
+    pslot_t *s = &PS[slot]; const long n = nc << PD; plain_reserve(s, n); s->n = n;
+    if(nc <= 0) return;
+    signed char *hk = s->hK; const int D = PD;
+    #pragma omp parallel for schedule(static)
+    for(long c = 0; c < nc; c++) for(int d = 0; d < D; d++) hk[c*D + d] = (signed char)cells[c*stride + d];
+    CKX(cudaMemcpyAsync(s->dK, hk, nc*D, cudaMemcpyHostToDevice, s->st));
+    if(skip){ memcpy(s->hS, skip, nc); CKX(cudaMemcpyAsync(s->dS, s->hS, nc, cudaMemcpyHostToDevice, s->st)); }
+    plain_launch(s, n, nc, 1, st, skip != NULL);
+    CKX(cudaMemcpyAsync(s->hF, s->dF, n*sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CKX(cudaMemcpyAsync(s->hA, s->dA, n*sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CKX(cudaEventRecord(s->ev, s->st));
+}
+
+extern "C" void gpu_wait(int slot, const double **fw, const double **abw){
+    pslot_t *s = &PS[slot];
+    if(s->n > 0) CKX(cudaEventSynchronize(s->ev));
+    *fw = s->hF; *abw = s->hA;
+}
+
+/* the reference's per-graph launcher (sq_gpu_launch_t, driver/gpu.h:18-19) on device buffers: int16
+ * coordinates, stride D, n points (cells: n = nc << D) */
+extern "C" void sqb_gg_launch(const sqb_graph_t *g, void *st, long n, const short *k, const unsigned char *skip,
+                              const double *EX, int K, double H, double *of, double *oab, int cmode, int cst){
+    if(n <= 0) return;
+    if(!G.on && sqb_dev_init(0)){ fprintf(stderr, "gpu: %s\n", g_err); exit(3); }
+    sqb_eval_t a; memset(&a, 0, sizeof a);
+    a.pts = k; a.n = cmode ? (n >> g->D) : n; a.esize = 2; a.stride = g->D; a.flag_at = -1; a.cells = cmode; a.st = cst;
+    a.X = EX; a.Wt = NULL; a.K = K; a.H = H; a.raw = 1; a.skip = skip; a.v = of; a.ab = oab;
+    size_t smem = 2*(2*K + 1)*sizeof(double);
+    g->f64(&a, grid_for(g, 0, n, smem), 128, smem, st);
+}
+
+/* pointwise evaluation (parity checks): n points given by their variables, FP64 (SQ_AB = ab) or
+ * double-double; f, abs_ hold n values (FP64) or n (hi, lo) pairs (double-double) */
+extern "C" int sqb_eval_points_impl(const sqb_graph_t *g, long n, const double *sf, int prec, int ab, double *f, double *abs_){
+    if(n <= 0) return 0;
+    const int D = g->D;
+    double *dsf = NULL, *dv = NULL, *dab = NULL, *dvl = NULL, *dabl = NULL; unsigned char *dsk = NULL;
+    CKR(cudaMalloc(&dsf, n*D*sizeof(double))); CKR(cudaMalloc(&dv, n*sizeof(double))); CKR(cudaMalloc(&dab, n*sizeof(double)));
+    CKR(cudaMalloc(&dvl, n*sizeof(double))); CKR(cudaMalloc(&dabl, n*sizeof(double))); CKR(cudaMalloc(&dsk, n));
+    CKR(cudaMemcpy(dsf, sf, n*D*sizeof(double), cudaMemcpyHostToDevice));
+    CKR(cudaMemset(dsk, ab ? 0 : 1, n));
+    double one = 1.0, *dX = NULL; CKR(cudaMalloc(&dX, sizeof(double))); CKR(cudaMemcpy(dX, &one, sizeof one, cudaMemcpyHostToDevice));
+    sqb_eval_t a; memset(&a, 0, sizeof a);
+    a.pts = NULL; a.n = n; a.esize = 1; a.stride = D; a.flag_at = -1; a.cells = 0;
+    a.X = dX; a.Wt = dX; a.K = 0; a.raw = 1; a.skip = dsk; a.v = dv; a.ab = dab; a.sfin = dsf; a.vlo = dvl; a.ablo = dabl;
+    size_t smem = 2*sizeof(double);
+    if(prec == 0) g->f64(&a, grid_for(g, 0, n, smem), 128, smem, G.s);
+    else { sqb_dd_t d; memset(&d, 0, sizeof d); d.e = a; d.all = 1; d.uu = dvl; g->dd(&d, grid_for(g, 1, n, smem), 128, smem, G.s); }
+    CKR(cudaGetLastError());
+    CKR(cudaStreamSynchronize(G.s));
+    if(prec == 0){
+        CKR(cudaMemcpy(f, dv, n*sizeof(double), cudaMemcpyDeviceToHost));
+        CKR(cudaMemcpy(abs_, dab, n*sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+        double *h = (double*)malloc(4*n*sizeof(double));
+        CKR(cudaMemcpy(h, dv, n*sizeof(double), cudaMemcpyDeviceToHost));
+        CKR(cudaMemcpy(h + n, dvl, n*sizeof(double), cudaMemcpyDeviceToHost));
+        CKR(cudaMemcpy(h + 2*n, dab, n*sizeof(double), cudaMemcpyDeviceToHost));
+        CKR(cudaMemcpy(h + 3*n, dabl, n*sizeof(double), cudaMemcpyDeviceToHost));
+        for(long i = 0; i < n; i++){ f[2*i] = h[i]; f[2*i + 1] = h[n + i]; abs_[2*i] = h[2*n + i]; abs_[2*i + 1] = h[3*n + i]; }
+        free(h);
+    }
+    cudaFree(dsf); cudaFree(dv); cudaFree(dab); cudaFree(dvl); cudaFree(dabl); cudaFree(dsk); cudaFree(dX);
+    return 0;
+}

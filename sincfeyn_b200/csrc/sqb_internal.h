@@ -1,0 +1,73 @@
+/* sqb_internal.h -- what the generated per-graph translation units and the runtime share: the launch
+ * arguments of the evaluation kernels and the graph descriptor with its launchers.  Not part of the
+ * public C ABI (include/sincfeyn_b200.h). */
+#pragma once
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status bits of one evaluated point (test mode) */
+enum {
+    SQB_PRESENT = 1,      /* a lattice node (not a child below the box) */
+    SQB_NEAR = 2,         /* |.| bound above NEARF*ABSERR: its children must check (driver/eval.c:37) */
+    SQB_FALLBACK = 4,     /* |.| bound above ABSERR: recomputed in double-double (driver/eval.c:38) */
+    SQB_UNRES = 8,        /* unresolved even in double-double (driver/eval.c:28) */
+    SQB_SKIPPED = 16      /* evaluated without the |.| sums (driver/eval.c:35) */
+};
+
+/* One launch of the FP64 evaluation kernel over nodes, or over the 2^D children of cells.
+ * Coordinates are integers k (|k| <= K) of esize bytes (1: the pt_t layout of the level lists and
+ * checkpoints, 2: the int16 layout of the reference's GPU plug-in), stride elements per node or
+ * cell; the per-node flags byte (pt_t slot PFLAG) sits at element flag_at, or flag_at < 0. */
+typedef struct {
+    const void *pts;
+    long n;                       /* nodes, or cells */
+    int esize, stride, flag_at;
+    int cells, st;                /* cells: child b of cell c is k_d - st*bit_d(b) (driver/sum.c:407) */
+    const double *X, *Wt;         /* 2K+1 entries: integration variable and weight factor per k;
+                                     Wt == NULL: the factor is X*H (driver/lattice.c:33) */
+    int K;
+    double H;
+    int raw;                      /* 1: plain form, v = f w and ab = ab w, no tests */
+    const unsigned char *skip;    /* per node or cell: evaluate without the |.| sums (may be NULL) */
+    int abskip, abcheck;          /* with flag_at >= 0: skip = abskip && (flags & 1) */
+    double abserr, near_thr, ddslack;
+    double *v, *ab;               /* value per point (raw: f w); raw only: ab w */
+    const double *sfin;           /* raw only, pointwise checks: the D variables of point i at sfin[i*D], w = 1 */
+    double *vlo, *ablo;           /* raw double-double pass: the low parts of f and ab */
+    unsigned char *stt;           /* test mode: status per point */
+    long *fb;                     /* test mode: points that need the fallback (unordered) */
+    unsigned long long *nfb;
+    long fbcap;
+} sqb_eval_t;
+
+/* The double-double kernel over a list of points of the same launch geometry (fb/nfb from the FP64
+ * pass), or over every point (all = 1: the all-double-double form). */
+typedef struct {
+    sqb_eval_t e;                 /* geometry, tables, outputs v and stt */
+    const long *list;             /* NULL with all = 1 */
+    const unsigned long long *nlist;
+    long listcap;
+    int all;
+    int dropunres;
+    double *uu;                   /* per point: e^2 of the round column (driver/eval.c:26) */
+} sqb_dd_t;
+
+typedef struct {
+    int regs, local_bytes, max_threads, blocks_per_sm;
+} sqb_kattr_t;
+
+typedef struct {
+    const char *name, *volkov;
+    int L, D, weight, n, fixed;
+    int zlattice;                              /* 1: the variable is z itself (synthetic integrand) */
+    void (*f64)(const sqb_eval_t *a, int grid, int block, size_t smem, void *stream);
+    void (*dd)(const sqb_dd_t *a, int grid, int block, size_t smem, void *stream);
+    /* which: 0 FP64 kernel, 1 dd kernel; blocks_per_sm for this block size and dynamic shared memory */
+    int (*attr)(int which, int block, size_t smem, sqb_kattr_t *out);
+} sqb_graph_t;
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,180 @@
+/* sqkern.cuh -- the evaluation kernels, instantiated once per graph by the generated translation
+ * unit (kgen output included after this header, then SQ_GRAPH(...) below).
+ *
+ * One thread per lattice point.  A point is a node (k given) or child b of a cell (k_d - st*bit_d(b),
+ * in the order of prep() in the reference, driver/sum.c:405-408; children below the box, k_d < -K,
+ * are not points).  The per-coordinate tables X[k+K] (the integration variable, s = e^{kh}) and
+ * Wt[k+K] (its weight factor s*h) sit in shared memory; the weight is accumulated in coordinate order
+ * as lattice_node() does (driver/lattice.c:30-34), so it rounds identically.
+ *
+ * FP64 pass (sqb_k_f64): f and the |.| sum in double.  Raw mode returns f*w and ab*w (the reference's
+ * GPU plug-in contract, driver/gpu_kernel.h:22-36).  Test mode applies the reference's per-point tests
+ * (finish(), driver/eval.c:33-53): skipped points keep f*w; otherwise the bound ab*w*16*eps/DDSLACK sets
+ * the near flag and, above ABSERR, queues the point for the double-double pass.
+ * DD pass (sqb_k_dd): the queued points (or all of them) in double-double, with qvalue()'s round
+ * column and unresolved-point rule (driver/eval.c:25-30). */
+#pragma once
+#include <cuda_runtime.h>
+#include <float.h>
+#include <math.h>
+#include "sqdd.cuh"
+#include "sqb_internal.h"
+
+#define SQ_TABLE static __constant__ const
+#define SQ_FUNC __device__
+#define SQ_CHUNK __device__ __noinline__
+#define RABS(x) sq_rabs(x)
+
+#ifndef SQB_BLOCK
+#define SQB_BLOCK 128
+#endif
+#define SQB_QEPS 4.93e-32   /* double-double epsilon of the fallback's error model (driver/common.h:8) */
+
+/* coordinates and weight of point i; returns false for a child below the box */
+template<int D>
+__device__ __forceinline__ bool sqb_point(const sqb_eval_t &a, const double *sX, const double *sW,
+                                          long i, long *cell, double *sf, double *w){
+    long c; int b;
+    if(a.cells){ c = i >> D; b = (int)(i & ((1L << D) - 1)); } else { c = i; b = 0; }
+    *cell = c;
+    if(a.sfin){
+#pragma unroll
+        for(int d = 0; d < D; d++) sf[d] = a.sfin[i*D + d];
+        *w = 1.0;
+        return true;
+    }
+    double ww = 1.0; bool in = true;
+    if(a.esize == 1){
+        const signed char *p = (const signed char*)a.pts + c*(long)a.stride;
+#pragma unroll
+        for(int d = 0; d < D; d++){
+            int kd = p[d] - (((b >> d) & 1) ? a.st : 0);
+            if(kd < -a.K){ in = false; kd = -a.K; }
+            sf[d] = sX[kd + a.K]; ww = ww*sW[kd + a.K];
+        }
+    } else {
+        const short *p = (const short*)a.pts + c*(long)a.stride;
+#pragma unroll
+        for(int d = 0; d < D; d++){
+            int kd = p[d] - (((b >> d) & 1) ? a.st : 0);
+            if(kd < -a.K){ in = false; kd = -a.K; }
+            sf[d] = sX[kd + a.K]; ww = ww*sW[kd + a.K];
+        }
+    }
+    *w = ww;
+    return in;
+}
+
+template<int D>
+__device__ __forceinline__ int sqb_skip(const sqb_eval_t &a, long c){
+    if(a.skip) return a.skip[c];
+    if(a.flag_at >= 0 && a.abskip){
+        int fl = a.esize == 1 ? ((const signed char*)a.pts)[c*(long)a.stride + a.flag_at]
+                              : ((const short*)a.pts)[c*(long)a.stride + a.flag_at];
+        return fl & 1;
+    }
+    return 0;
+}
+
+__device__ __forceinline__ void sqb_tables(const sqb_eval_t &a, double *sX, double *sW){
+    const int nt = 2*a.K + 1;
+    for(int j = threadIdx.x; j < nt; j += blockDim.x){ sX[j] = a.X[j]; sW[j] = a.Wt ? a.Wt[j] : a.X[j]*a.H; }
+    __syncthreads();
+}
+
+template<class F, int D>
+__global__ void __launch_bounds__(SQB_BLOCK) sqb_k_f64(const sqb_eval_t a){
+    extern __shared__ double sqb_sm[];
+    double *sX = sqb_sm, *sW = sqb_sm + (2*a.K + 1);
+    sqb_tables(a, sX, sW);
+    const long n = a.cells ? (a.n << D) : a.n;
+    for(long i = blockIdx.x*(long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x*blockDim.x){
+        long c; double sf[D], w;
+        const bool in = sqb_point<D>(a, sX, sW, i, &c, sf, &w);
+        if(!in){
+            a.v[i] = 0;
+            if(a.raw) a.ab[i] = 0; else a.stt[i] = 0;
+            continue;
+        }
+        const int sk = sqb_skip<D>(a, c);
+        const bool noab = sk && !a.abcheck;
+        double ab = 0, f;
+        if(noab) f = F::template f<double, 0>(sf, &ab);
+        else     f = F::template f<double, 1>(sf, &ab);
+        const double fw = f*w;
+        if(a.raw){ a.v[i] = fw; a.ab[i] = ab*w; continue; }
+        unsigned char s = SQB_PRESENT | (sk ? SQB_SKIPPED : 0);
+        double v;
+        if(noab) v = isfinite(fw) ? fw : 0.0;
+        else {
+            const double bnd = ab*w*16*DBL_EPSILON/a.ddslack;
+            if(!(bnd <= a.near_thr)) s |= SQB_NEAR;
+            if(!(bnd <= a.abserr)){
+                s |= SQB_FALLBACK; v = 0.0;
+                const unsigned long long q = atomicAdd(a.nfb, 1ULL);
+                if((long)q < a.fbcap) a.fb[q] = i;
+            } else v = isfinite(fw) ? fw : 0.0;
+        }
+        a.v[i] = v; a.stt[i] = s;
+    }
+}
+
+template<class F, int D>
+__global__ void __launch_bounds__(SQB_BLOCK) sqb_k_dd(const sqb_dd_t a){
+    extern __shared__ double sqb_sm[];
+    const sqb_eval_t &e = a.e;
+    double *sX = sqb_sm, *sW = sqb_sm + (2*e.K + 1);
+    sqb_tables(e, sX, sW);
+    long n;
+    if(a.all) n = e.cells ? (e.n << D) : e.n;
+    else { n = (long)*a.nlist; if(n > a.listcap) n = a.listcap; }
+    for(long j = blockIdx.x*(long)blockDim.x + threadIdx.x; j < n; j += (long)gridDim.x*blockDim.x){
+        const long i = a.all ? j : a.list[j];
+        long c; double sf[D], w;
+        if(!sqb_point<D>(e, sX, sW, i, &c, sf, &w)){ e.v[i] = 0; e.stt[i] = 0; a.uu[i] = 0; continue; }
+        sqdd sq[D], abq;
+#pragma unroll
+        for(int d = 0; d < D; d++) sq[d] = sqdd(sf[d]);
+        const sqdd vq = F::template f<sqdd, 1>(sq, &abq);
+        if(e.raw){ e.v[i] = vq.hi; e.vlo[i] = vq.lo; e.ab[i] = abq.hi; e.ablo[i] = abq.lo; continue; }
+        const double vqd = vq.value(), abqd = abq.value();
+        /* qvalue(), driver/eval.c:25-30 */
+        const double ee = abqd*w*SQB_QEPS;
+        const double u = !(ee*16 <= e.abserr) ? (isfinite(ee) ? ee*ee : 0.0) : 0.0;
+        double v = isfinite(vqd) ? vqd*w : 0.0;
+        unsigned char s;
+        if(a.all){
+            /* the all-double-double form: the near flag from the double-double |.| sum */
+            s = SQB_PRESENT | SQB_FALLBACK | (sqb_skip<D>(e, c) ? SQB_SKIPPED : 0);
+            if(!(abqd*w*16*DBL_EPSILON/e.ddslack <= e.near_thr)) s |= SQB_NEAR;
+        } else s = e.stt[i];
+        if(!(ee <= fabs(v))){ s |= SQB_UNRES; if(a.dropunres) v = 0.0; }
+        e.v[i] = v; e.stt[i] = s; a.uu[i] = u;
+    }
+}
+
+/* SQ_GRAPH(name, volkov, L, D, weight, n, fixed): the generated file ends with it, after namespace
+ * sqg_<name> with the class template K<Real, SQ_AB> holding f_<name>. */
+#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
+namespace sqg_##NAME {                                                                             \
+struct F {                                                                                         \
+    template<class R, int AB> static __device__ __forceinline__ R f(const R *sf, R *ab){           \
+        return K<R, AB>::f_##NAME(sf, ab); }                                                       \
+};                                                                                                 \
+static void f64(const sqb_eval_t *a, int grid, int block, size_t smem, void *st){                  \
+    sqb_k_f64<F, D><<<grid, block, smem, (cudaStream_t)st>>>(*a); }                                \
+static void dd(const sqb_dd_t *a, int grid, int block, size_t smem, void *st){                     \
+    sqb_k_dd<F, D><<<grid, block, smem, (cudaStream_t)st>>>(*a); }                                 \
+static int attr(int which, int block, size_t smem, sqb_kattr_t *o){                                \
+    cudaFuncAttributes fa; int nb = 0;                                                             \
+    cudaError_t e = which ? cudaFuncGetAttributes(&fa, sqb_k_dd<F, D>)                             \
+                          : cudaFuncGetAttributes(&fa, sqb_k_f64<F, D>);                           \
+    if(e != cudaSuccess) return 0;                                                                 \
+    e = which ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sqb_k_dd<F, D>, block, smem)    \
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sqb_k_f64<F, D>, block, smem);  \
+    if(e != cudaSuccess) return 0;                                                                 \
+    o->regs = fa.numRegs; o->local_bytes = (int)fa.localSizeBytes;                                 \
+    o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; return 1; }                     \
+}                                                                                                  \
+extern "C" const sqb_graph_t SQB_##NAME = {#NAME, VOLKOV, L, D, W, NP, FIX, 0,                     \
+    sqg_##NAME::f64, sqg_##NAME::dd, sqg_##NAME::attr};

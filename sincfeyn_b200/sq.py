@@ -1,0 +1,175 @@
+"""Python mirror of the evaluator's C ABI (include/sincfeyn_b200.h), over ctypes.
+
+The library is sincfeyn_b200/lib/libsqb200.so, built in-tree by sincfeyn_b200.build.  There is no other
+implementation behind these functions: if the library is missing, or the CUDA device cannot be used,
+they raise.
+
+    import sincfeyn_b200.sq as sq
+    r = sq.hsum('g2_00', 1.0, 97, 1e-12)          # the reference's hsum() for one graph
+    rows = sq.run(1.0, 97, 1e-12, ['all2'])       # `sincqed run 1.0 97 1e-12 all2`, one row per graph
+"""
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'lib', 'libsqb200.so')
+_lib = None
+
+
+class Opts(C.Structure):
+    """sqb_opts_t: the reference's environment settings that reach the hot path (driver/main.c:176-185)."""
+    _fields_ = [('abserr0', C.c_double), ('abrel', C.c_double), ('nearf', C.c_double), ('ddslack', C.c_double),
+                ('abskip', C.c_int), ('abcheck', C.c_int), ('dropunres', C.c_int), ('growskip', C.c_int),
+                ('alldd', C.c_int), ('device', C.c_int), ('max_children', C.c_long), ('verbose', C.c_int)]
+
+
+class Result(C.Structure):
+    """sqb_result_t: res_t of the reference (driver/sq.h:111) plus the log counters and timings."""
+    _fields_ = [('S', C.c_double * 3), ('Ah', C.c_double), ('ref', C.c_double), ('prune', C.c_double),
+                ('trunc', C.c_double), ('unres', C.c_double), ('t', C.c_double),
+                ('nev', C.c_long), ('nq', C.c_long), ('kept_top', C.c_long),
+                ('es1', C.c_double), ('es2', C.c_double), ('esok', C.c_int),
+                ('abskipped', C.c_long), ('unresdrop', C.c_long), ('zero', C.c_int),
+                ('t_top', C.c_double), ('t_levels', C.c_double), ('nlev', C.c_int),
+                ('lev_evals', C.c_long * 16), ('lev_ms', C.c_double * 16)]
+
+
+class SqbError(RuntimeError):
+    pass
+
+
+def lib():
+    """The loaded C-ABI library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SqbError('%s is missing: build it with `python -m sincfeyn_b200.build`' % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        L.sqb_default_opts.argtypes = [C.POINTER(Opts)]
+        L.sqb_hsum.argtypes = [C.c_char_p, C.c_double, C.c_int, C.c_double, C.c_int, C.POINTER(Opts), C.POINTER(Result)]
+        L.sqb_hsum.restype = C.c_int
+        L.sqb_error.restype = C.c_char_p
+        L.sqb_graph_count.restype = C.c_int
+        L.sqb_graph_name.argtypes = [C.c_int]
+        L.sqb_graph_name.restype = C.c_char_p
+        L.sqb_graph_volkov.argtypes = [C.c_char_p]
+        L.sqb_graph_volkov.restype = C.c_char_p
+        L.sqb_graph_info.argtypes = [C.c_char_p, C.POINTER(C.c_int)]
+        L.sqb_graph_flops.argtypes = [C.c_char_p, C.c_int]
+        L.sqb_graph_flops.restype = C.c_double
+        L.sqb_eval_points.argtypes = [C.c_char_p, C.c_long, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        L.sqb_eval_points.restype = C.c_int
+        L.sqb_device_info.restype = C.c_char_p
+        L.gpu_info.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def default_opts(**kw):
+    o = Opts()
+    lib().sqb_default_opts(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def graphs():
+    """[{name, volkov, L, D, weight, n, fixed}] of the graphs compiled into the library, in registry order."""
+    L = lib()
+    out = []
+    for i in range(L.sqb_graph_count()):
+        name = L.sqb_graph_name(i)
+        info = (C.c_int * 6)()
+        L.sqb_graph_info(name, info)
+        out.append(dict(name=name.decode(), volkov=L.sqb_graph_volkov(name).decode(), L=info[0], D=info[1],
+                        weight=info[2], n=info[3], fixed=info[4]))
+    return out
+
+
+def flops(name, ab=1):
+    """Algorithmic FP64 flops per point of the graph's double path (with or without the |.| sums)."""
+    return lib().sqb_graph_flops(name.encode(), int(ab))
+
+
+def default_top(h):
+    """driver/main.c:211-215 (SINCQED_TOPSTEP = 3)."""
+    top = 1
+    while top < 2 and (1 << (top + 1)) * h <= 3.0 * (1 + 1e-9):
+        top += 1
+    return top
+
+
+def hsum(graph, h, N, eps, top=-1, **opts):
+    """The hierarchical Sinc sum of one graph; returns the result fields as a dict."""
+    o = default_opts(**opts)
+    r = Result()
+    rc = lib().sqb_hsum(graph.encode(), float(h), int(N), float(eps), int(top), C.byref(o), C.byref(r))
+    if rc:
+        raise SqbError('%s: %s' % (graph, lib().sqb_error().decode()))
+    d = {f: getattr(r, f) for f, _ in Result._fields_}
+    d['S'] = list(r.S)
+    d['lev_evals'] = list(r.lev_evals)[:r.nlev]
+    d['lev_ms'] = list(r.lev_ms)[:r.nlev]
+    return d
+
+
+def select(selectors):
+    """Graph names matched by names, Volkov strings or groups (driver/graphs.c:15-29), in order."""
+    gs = graphs()
+
+    def hit(g, s):
+        n = g['name']
+        if s in (n, g['volkov']):
+            return True
+        return {'all2': g['L'] == 2, 'all3': g['L'] == 3 and not n.startswith('w3_'), 'all4': g['L'] == 4,
+                'q3': n.startswith('g3_') and n != 'g3_lbl', 'vp3': n.startswith('v3_'),
+                'vp4': n.startswith('v4_') or n.startswith('w4_'), 'lbl': n == 'g3_lbl'}.get(s, False)
+    out = []
+    for s in selectors:
+        for g in gs:
+            if hit(g, s) and g['name'] not in out:
+                out.append(g['name'])
+    return out
+
+
+def run(h, N, eps, selectors, top=-1, **opts):
+    """`sincqed run h N eps [top] GRAPH...`: per graph its value (weight * S_h) and error columns, as the
+    reference's run_graph() computes them (driver/main.c:40-75)."""
+    if top < 0:
+        top = default_top(h)
+    info = {g['name']: g for g in graphs()}
+    rows = []
+    for name in select(selectors):
+        r = hsum(name, h, N, eps, top, **opts)
+        w = info[name]['weight']
+        S0, S1 = r['S'][0], r['S'][1]
+        d2 = abs(S1 - S0) if not math.isnan(S1) else float('nan')
+        disc = 2 * d2 * d2 / r['Ah'] if r['Ah'] > 0 else 0.0
+        err = w * (disc + r['prune'] + r['trunc'] + r['unres'])
+        rows.append(dict(name=name, D=info[name]['D'], weight=w, value=w * S0, err=err, disc=w * disc,
+                         prune=w * r['prune'], trunc=w * r['trunc'], round=w * r['unres'],
+                         S_2h=w * S1, evals=r['nev'], quad=r['nq'], kept=r['kept_top'], time=r['t'], raw=r))
+    return rows
+
+
+def eval_points(graph, sf, prec=0, ab=1):
+    """The graph kernel at the points sf (n x D) on the device.  prec 0: FP64 (f, ab) arrays; prec 1:
+    double-double, (f, ab) as (n, 2) arrays of (hi, lo)."""
+    sf = np.ascontiguousarray(sf, dtype=np.float64)
+    n = sf.shape[0]
+    if prec == 0:
+        f = np.empty(n)
+        a = np.empty(n)
+    else:
+        f = np.empty((n, 2))
+        a = np.empty((n, 2))
+    rc = lib().sqb_eval_points(graph.encode(), n, sf.ctypes.data, int(prec), int(ab), f.ctypes.data, a.ctypes.data)
+    if rc:
+        raise SqbError('%s: %s' % (graph, lib().sqb_error().decode()))
+    return f, a
+
+
+def device_info():
+    return lib().sqb_device_info().decode()

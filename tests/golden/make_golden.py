@@ -1,0 +1,84 @@
+#!/usr/bin/env python3
+"""Writes the golden fixtures in tests/golden/ from the reference itself (oracle/_ref, built by
+oracle/Makefile from the reference sources).  Run from the repository root after `make -C oracle`:
+
+    python tests/golden/make_golden.py
+
+Fixtures
+  all2_h1.0_N97_eps1e-12.json   `sincqed run 1.0 97 1e-12 all2`, the reference CPU build as shipped
+                                (symmetry fold on) and the -ffp-contract=off build with SINCQED_SYM=0 (the
+                                unfolded point set the GPU evaluates, driver/sum.c:571): every column of
+                                every results line
+  boxsum_gl.json                the reference's pointwise known-answer program
+                                (mathematica/check/boxsum_gl.c): term values at k = 0 and k = (1,-1,2,0),
+                                h = 1, and full-box sums at h = 1, K = 6, for the five two-loop kernels
+  pointwise_<class>.npz         400 (g3: 128) seeded nodes per graph, sigma = e^z, z ~ U[-3,3] (the protocol of
+                                tests/check_onept.sh): fd with SQ_AB = 1 and 0 and fq (hi, lo) of the
+                                reference kernels
+"""
+import json
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+import refpy  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def all2():
+    d = {'command': 'run 1.0 97 1e-12 all2'}
+    rows, _ = refpy.run(refpy.SINCQED, 1.0, 97, 1e-12, ['all2'])
+    d['reference'] = rows
+    rows, _ = refpy.run(refpy.SINCQED_EXACT, 1.0, 97, 1e-12, ['all2'], env={'SINCQED_SYM': '0'})
+    d['reference_exact_unfolded'] = rows
+    for r in d['reference'] + d['reference_exact_unfolded']:
+        r.pop('time_s', None)
+    with open(os.path.join(OUT, 'all2_h1.0_N97_eps1e-12.json'), 'w') as f:
+        json.dump(d, f, indent=1)
+
+
+def boxsum():
+    out = subprocess.run([refpy.BOXSUM, '1.0', '6'], stdout=subprocess.PIPE, text=True, check=True).stdout
+    d = {}
+    for line in out.splitlines():
+        m = re.match(r'(\w+) term0 (\S+) term1 (\S+)', line)
+        if m:
+            d.setdefault(m.group(1), {}).update(term0=float(m.group(2)), term1=float(m.group(3)))
+        m = re.match(r'(\w+) box h=1.0 K=6 (\S+)', line)
+        if m:
+            d.setdefault(m.group(1), {}).update(box_h1_K6=float(m.group(2)))
+    d['_source'] = 'mathematica/check/boxsum_gl.c run as `boxsum_gl 1.0 6` (QREAL_DOUBLE)'
+    with open(os.path.join(OUT, 'boxsum_gl.json'), 'w') as f:
+        json.dump(d, f, indent=1)
+
+
+def pointwise(cls, prefixes, npts=400):
+    rng = np.random.default_rng(12345)
+    arrays = {}
+    for name in refpy.names():
+        if not name.startswith(prefixes):
+            continue
+        D = refpy.info(name)['D']
+        sf = np.exp(rng.uniform(-3, 3, size=(npts, D)))
+        f1, a1 = refpy.fd(name, sf, 1)
+        f0, a0 = refpy.fd(name, sf, 0)
+        q, qa = refpy.fq(name, sf)
+        arrays[name + '.sf'] = sf
+        arrays[name + '.fd1'] = np.stack([f1, a1], 1)
+        arrays[name + '.fd0'] = np.stack([f0, a0], 1)
+        arrays[name + '.fq'] = np.concatenate([q, qa], 1)
+    np.savez_compressed(os.path.join(OUT, 'pointwise_%s.npz' % cls), **arrays)
+
+
+if __name__ == '__main__':
+    all2()
+    boxsum()
+    pointwise('g2', ('g2_', 'v2_'))
+    pointwise('v3', ('v3_', 'w3_'))
+    pointwise('g3', ('g3_',), 128)

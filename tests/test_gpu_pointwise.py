@@ -1,0 +1,44 @@
+"""Pointwise parity of the sm_100a kernels with the reference kernels (GPU).
+
+At the seeded nodes of the golden fixtures (the tests/check_onept.sh protocol: sigma = e^z, z ~ U[-3,3])
+the device FP64 kernels (nvcc -fmad=false) must give the reference double half's f and |.| sum bit for
+bit, for SQ_AB = 1 and 0, and the device double-double kernels the reference's double-double fq bit for
+bit.  The fixtures were written by the reference compiled with -ffp-contract=off
+(tests/golden/make_golden.py)."""
+import os
+
+import numpy as np
+import pytest
+
+from sincfeyn_b200 import sq
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+pytestmark = pytest.mark.gpu
+# see tests/test_codegen_host.py: FP64 agrees to 4 ulp of the |.| sum, double-double bit for bit
+NOT_BITWISE = {'g3_lbl'}
+
+
+@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3'])
+def test_fp64_and_dd_bitwise(cls):
+    z = np.load(os.path.join(GOLD, 'pointwise_%s.npz' % cls))
+    have = {g['name'] for g in sq.graphs()}
+    names = sorted({k.split('.')[0] for k in z.files} & have)
+    if not names:
+        pytest.skip('class %s not in this build' % cls)
+    bad = []
+    for n in names:
+        sf = z[n + '.sf']
+        for ab, key in ((1, '.fd1'), (0, '.fd0')):
+            f, a = sq.eval_points(n, sf, 0, ab)
+            w = z[n + key]
+            if n in NOT_BITWISE:
+                tol = 4*np.finfo(float).eps*z[n + '.fd1'][:, 1]
+                if not (np.all(np.abs(f - w[:, 0]) <= tol) and (not ab or np.all(np.abs(a - w[:, 1]) <= 1e-12*w[:, 1]))):
+                    bad.append((n, 'fp64 tolerance', ab))
+                continue
+            if not np.array_equal(f, w[:, 0], equal_nan=True) or (ab and not np.array_equal(a, w[:, 1], equal_nan=True)):
+                bad.append((n, 'fp64', ab, float(np.nanmax(np.abs(f - w[:, 0]) / np.maximum(w[:, 1], 1e-300)))))
+        f, a = sq.eval_points(n, sf, 1, 1)
+        if not np.array_equal(np.concatenate([f, a], 1), z[n + '.fq'], equal_nan=True):
+            bad.append((n, 'dd'))
+    assert not bad, bad
