@@ -1,0 +1,282 @@
+#!/usr/bin/env python3
+"""Benchmark of the evaluator on its headline workload: the three-loop set (all3: 41 integrals, 72
+diagrams) at h = 0.7, N = 139 (K rounded up to 72, top = 2), eps = 1e-12, FP64 with the double-double
+fallback on the device.  Metric: integrand points per second and time-to-sum.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one integral's whole hierarchical sum through the public C ABI (sqb_hsum): the top-level
+grow and dilation, then every refinement level on the device.  The timed steps walk the set in a fixed
+order (registry order); K defaults to the whole set, so the timed region is the set's time-to-sum.
+The W warm-up steps run the first W integrals untimed.  With N ranks (torchrun) the integrals are dealt
+round-robin to the ranks (strong scaling, no collective on the data path); the time is the maximum
+over ranks.
+
+JSON line (rank 0):
+  value      points/s of the device-resident refinement levels: evaluated children / device time of the
+             level passes (cell lists already in HBM when each pass starts; CUDA events on the library's
+             stream)
+  e2e        points/s through sqb_hsum with host-side parameters and host-side results, every host<->device
+             copy inside (all evaluated points / device-timed steps); time_to_sum_s is the set's total
+  roofline   the FP64 evaluation kernels (sqb_k_f64<graph>): algorithmic flops per point (+ - * / of the
+             kernel's double path, counted by the code generator; skipped |.| sums counted as skipped) over
+             their event-timed launches, against this device's FP64 FMA rate measured by a probe kernel
+  cpu_baseline  the reference's own OpenMP CPU build (oracle/_ref/sincqed) on this host's cores, on a
+             bounded sample of the same workload
+  vs_alldd   the same sample of integrals in the plain all-double-double form, time ratio
+`--impl reference` times the reference CPU build on the same metric (rank 0 only).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+H, N_PTS, EPS = 0.7, 139, 1e-12
+SET = 'all3'
+# the CPU samples: three-loop integrals of D = 5, 5 and 6 at the workload's (h, N, eps)
+CPU_SAMPLE = ['g3_07', 'v3_01', 'g3_01']
+ALLDD_SAMPLE = ['v3_01', 'g3_07', 'g3_01']
+PROFILE_TRAFFIC = os.path.join(ROOT, 'profiles', 'fp64_kernel_traffic.json')
+
+
+def env_rank():
+    return int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1)), int(os.environ.get('LOCAL_RANK', 0))
+
+
+def assign(integrals, rank, world):
+    """Round-robin deal of the set's integrals to the ranks (each integral exactly once)."""
+    return [x for i, x in enumerate(integrals) if i % world == rank]
+
+
+def reduce_max_sum(vals_max, vals_sum, world):
+    """Max over ranks of vals_max and sum of vals_sum (torch.distributed all_reduce; identity at world 1)."""
+    if world == 1:
+        return list(vals_max), list(vals_sum)
+    import torch
+    import torch.distributed as dist
+    dev = 'cuda' if dist.get_backend() == 'nccl' else 'cpu'
+    a = torch.tensor(vals_max, dtype=torch.float64, device=dev)
+    b = torch.tensor(vals_sum, dtype=torch.float64, device=dev)
+    dist.all_reduce(a, op=dist.ReduceOp.MAX)
+    dist.all_reduce(b, op=dist.ReduceOp.SUM)
+    return a.cpu().tolist(), b.cpu().tolist()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, power, throttle reasons)."""
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile('w+', suffix='.csv', delete=False)
+        try:
+            self.p = subprocess.Popen(['nvidia-smi', '-i', str(index), '--query-gpu=' + self.Q, '--format=csv,noheader,nounits',
+                                       '-lms', '200'], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [l.split(', ') for l in self.f.read().strip().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace('.', '').isdigit()]
+        if not sm:
+            return None
+        reasons = set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.strip() == 'Active':
+                    reasons.add(n)
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': float(rows[0][2]), 'samples': len(sm),
+                'power_w_max': max(float(r[3]) for r in rows if len(r) > 3 and r[3].replace('.', '').isdigit()),
+                'reasons': sorted(reasons)}
+
+
+def cpu_reference(graphs, threads, budget_s=None):
+    """The reference CPU build (oracle/_ref/sincqed, symmetry fold on as shipped) on these integrals;
+    returns (evals, seconds, per-graph rows)."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import refpy
+    if not refpy.available():
+        raise RuntimeError('oracle/_ref/sincqed is not built')
+    ev, sec, rows = 0, 0.0, []
+    for g in graphs:
+        t0 = time.perf_counter()
+        r, _ = refpy.run(refpy.SINCQED, H, N_PTS, EPS, [g], threads=threads)
+        dt = time.perf_counter() - t0
+        ev += r[0]['evals']
+        sec += dt
+        rows.append({'graph': g, 'evals': r[0]['evals'], 'seconds': round(dt, 3), 'value': r[0]['value']})
+        if budget_s and sec > budget_s:
+            break
+    return ev, sec, rows
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's CPU implementation of the path, all host threads, one integral of
+    the CPU sample per step (cycling), same metric."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    seq = [CPU_SAMPLE[i % len(CPU_SAMPLE)] for i in range(args.warmup + args.steps)]
+    cpu_reference(seq[:args.warmup], threads)
+    ev, sec, rows = cpu_reference(seq[args.warmup:], threads)
+    v = ev/sec
+    line = {'impl': 'reference', 'metric': 'integrand points/s (time-to-sum) of the three-loop set at h=0.7',
+            'value': v, 'unit': 'points/s', 'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': 1e3*sec/args.steps, 'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None,
+            'dtype': 'f64+dd', 'data': 'the reference kernels (kernels/g3, kernels/v3), no external data',
+            'config': {'workload': 'all3 sample %s at h=%g N=%d eps=%g' % (','.join(CPU_SAMPLE), H, N_PTS, EPS),
+                       'cpu': 'oracle/_ref/sincqed (reference CPU build, OpenMP)'},
+            'cpu_baseline': {'value': v, 'unit': 'points/s', 'cores': threads, 'kind': 'reference',
+                             'sample': '%d integrals cycling over %s' % (args.steps, ','.join(CPU_SAMPLE))},
+            'e2e': {'value': v, 'unit': 'points/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=None, help='integrals timed (default: the whole set)')
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
+    ap.add_argument('--no-alldd', action='store_true', help='skip the all-double-double comparison')
+    args = ap.parse_args()
+    rank, world, local = env_rank()
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+    if args.impl == 'reference':
+        if args.steps is None:
+            args.steps = 41
+        run_reference(args, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from sincfeyn_b200 import sq
+    torch.cuda.set_device(local)
+    o = sq.default_opts(device=local)
+    names = sq.select([SET])
+    if args.steps is None:
+        args.steps = len(names)
+    order = [names[i % len(names)] for i in range(args.steps)]
+    mine = assign(order, rank, world)
+    L = sq.lib()
+    import ctypes as C
+    L.sqb_timer_stop.restype = C.c_double
+    L.sqb_l2_flush.argtypes = [C.c_size_t]
+    sq.kernel_timing(True)
+    # warm-up: the first W integrals of the set, untimed
+    for g in names[:args.warmup]:
+        sq.hsum(g, H, N_PTS, EPS, device=local)
+    peak = sq.probe_fp64(True)
+    flops = {g: (sq.flops(g, 1), sq.flops(g, 0)) for g in names}
+    weight = {x['name']: x['weight'] for x in sq.graphs()}
+    h0 = (C.c_ulonglong(), C.c_ulonglong())
+    L.sqb_copy_bytes(C.byref(h0[0]), C.byref(h0[1]))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    t_wall = time.perf_counter()
+    step_ms, lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches, results = 0.0, 0.0, 0, 0, 0.0, 0, 0.0, 0, []
+    for g in mine:
+        L.sqb_l2_flush(256 << 20)
+        L.sqb_timer_start()
+        r = sq.hsum(g, H, N_PTS, EPS, device=local)
+        ms = L.sqb_timer_stop()
+        step_ms += ms
+        lev_ms += sum(r['lev_ms'])
+        lev_ev += sum(r['lev_evals'])
+        nev += r['nev']
+        f64_ms += r['f64_ms']
+        f64_n += r['f64_launches']
+        launches += r['launches'] + 1
+        a1, a0 = flops[g]
+        fl += (r['nev'] - r['abskipped'])*a1 + r['abskipped']*a0
+        results.append([g, r['S'][0]*weight[g], r['nev'], r['nq'], round(ms, 2)])
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+    h1 = (C.c_ulonglong(), C.c_ulonglong())
+    L.sqb_copy_bytes(C.byref(h1[0]), C.byref(h1[1]))
+    mx, sm = reduce_max_sum([step_ms, wall], [lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches,
+                                              h1[0].value - h0[0].value, h1[1].value - h0[1].value], world)
+    step_ms, wall = mx
+    lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches, h2d, d2h = sm
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    achieved = fl/(f64_ms*1e-3)/1e12 if f64_ms > 0 else None
+    traffic = None
+    if os.path.exists(PROFILE_TRAFFIC):
+        with open(PROFILE_TRAFFIC) as f:
+            prof = json.load(f)
+        if f64_n:
+            traffic = prof['dram_bytes_per_point']*(lev_ev/max(1, f64_n))
+    line = {
+        'metric': 'integrand points/s (time-to-sum) of the three-loop set at h=0.7',
+        'value': lev_ev/(lev_ms*1e-3) if lev_ms > 0 else None, 'unit': 'points/s',
+        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': step_ms/max(1, len(mine)),
+        'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f64+dd',
+        'data': 'the reference kernels (kernels/g3, kernels/v3) as integrands; no external data',
+        'config': {'workload': '%s (%d integrals) h=%g N=%d eps=%g top=2, FP64 + double-double fallback'
+                               % (SET, len(names), H, N_PTS, EPS),
+                   'integrals_timed': args.steps, 'l2': 'flushed (256 MiB memset) before every step',
+                   'parallelism': 'integrals dealt round-robin over %d GPU(s)' % world},
+        'time_to_sum_s': step_ms*1e-3 if args.steps >= len(names) else None,
+        'e2e': {'value': nev/(step_ms*1e-3), 'unit': 'points/s', 'h2d_bytes_per_step': int(h2d/args.steps),
+                'd2h_bytes_per_step': int(d2h/args.steps), 'wall_s': wall},
+        'roofline': {'bound': 'fp64', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+                     'frac': achieved/peak if achieved else None, 'traffic': traffic,
+                     'kernel': 'sqb_k_f64<graph> (FP64 evaluation)',
+                     'peak_source': 'measured FP64 FMA rate (probe kernel, this device)',
+                     'flops_per_launch': fl/max(1, f64_n), 'launches': int(f64_n)},
+        'gpu_launches': int(launches),
+        'clocks': clk,
+        'points': int(nev), 'level_points': int(lev_ev),
+    }
+    if world == 1 and not args.no_cpu:
+        try:
+            ev, sec, rows = cpu_reference(CPU_SAMPLE, os.cpu_count() or 1, budget_s=30)
+            line['cpu_baseline'] = {'value': ev/sec, 'unit': 'points/s', 'cores': os.cpu_count() or 1, 'kind': 'reference',
+                                    'sample': 'reference CPU build on %s at h=%g N=%d eps=%g (%.1f s)'
+                                              % (','.join(r['graph'] for r in rows), H, N_PTS, EPS, sec)}
+        except Exception as e:                      # the oracle binary is test infrastructure; report why
+            line['cpu_baseline'] = {'value': None, 'unavailable': str(e)[:200]}
+    if world == 1 and not args.no_alldd:
+        t_f, t_d = 0.0, 0.0
+        for g in ALLDD_SAMPLE:
+            L.sqb_timer_start(); sq.hsum(g, H, N_PTS, EPS); t_f += L.sqb_timer_stop()
+            L.sqb_timer_start(); sq.hsum(g, H, N_PTS, EPS, alldd=1); t_d += L.sqb_timer_stop()
+        line['vs_alldd'] = {'sample': ALLDD_SAMPLE, 'fp64dd_s': t_f*1e-3, 'alldd_s': t_d*1e-3, 'speedup': t_d/t_f}
+    line['per_integral'] = {'columns': ['graph', 'value', 'evals', 'fallback', 'ms'], 'rows': results}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -15,6 +15,7 @@
  * except where the reference's plug-in contract does (CUDA errors and a D mismatch in the plain form,
  * driver/gpu.cu:16,59); the chosen form returns an error code and sqb_error() says why. */
 #pragma once
+#include <stddef.h>
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -78,6 +79,10 @@ typedef struct {
     int nlev;
     long lev_evals[16];
     double lev_ms[16];
+    /* with sqb_kernel_timing(1): milliseconds in the FP64 and double-double evaluation kernels, and the
+     * number of FP64 launches; always: kernels of this library launched by the call */
+    double f64_ms, dd_ms;
+    long f64_launches, launches;
 } sqb_result_t;
 
 void sqb_default_opts(sqb_opts_t *o);
@@ -103,6 +108,20 @@ int  sqb_eval_points(const char *graph, long n, const double *sf, int prec, int 
 
 /* the device the library runs on ("off" before the first call) */
 const char *sqb_device_info(void);
+
+/* instrumentation: bracket every FP64 and double-double evaluation launch with events (one
+ * synchronisation per batch) so that sqb_result_t carries their times; and the measured FP64 rate of
+ * this device in TFLOP/s (fma = 1: fused multiply-adds, 2 flops each; 0: adds), the roofline
+ * denominator of the evaluation kernels */
+void sqb_kernel_timing(int on);
+double sqb_probe_fp64(int fma, long iters);
+/* bytes copied host->device and device->host by the chosen form so far */
+void sqb_copy_bytes(unsigned long long *h2d, unsigned long long *d2h);
+/* CUDA events on the library's stream around a region of calls: device milliseconds */
+int  sqb_timer_start(void);
+double sqb_timer_stop(void);
+/* overwrite `bytes` of device memory on the library's stream (an L2 flush between timed steps) */
+int  sqb_l2_flush(size_t bytes);
 
 #ifdef __cplusplus
 }

@@ -6,15 +6,18 @@
  *   box_zero     4097 fixed probe nodes; an integrand that is 0 at all of them is reported as zero
  *                (driver/sum.c:346-359);
  *   grow         the support-following top level (driver/sumkey.h:126-461): breadth-first from z = 0
- *                over axis neighbours at step 2^top h; a frontier is evaluated as one device batch;
- *                the running threshold eps_rel * sum|f w|; the next frontier is every not-yet-seen
+ *                over axis neighbours at step 2^top h; a frontier is evaluated as one device batch,
+ *                its values come to the host for the order-dependent sums (Neumaier S, the running
+ *                sum|f w| whose threshold eps_rel * a decides what is kept, the outer shells, the
+ *                dropped weight), and the device builds the next frontier: every not-yet-seen
  *                neighbour of a kept point, in (kept point, axis, sign) order -- the order the
- *                reference's parallel lowest-id claims produce; then the final re-threshold and the
- *                shadow-tier flood fill.  One table holds every evaluated point, which is the
- *                reference's result whenever it reports no candidate below its freed boundary
- *                tables (BTUNS = 0, driver/sum.c:631);
- *   dilate       the kept cells and their axis neighbours, deduplicated (skip bit AND, tier max) and
- *                sorted by mixed-radix key, i.e. lexicographically in k (driver/sumkey.h:20-90);
+ *                reference's parallel lowest-id claims produce (topgrid.cu); then the final
+ *                re-threshold and the shadow-tier flood fill on the device.  One table holds every
+ *                evaluated point, which is the reference's result whenever it reports no candidate
+ *                below its freed boundary tables (BTUNS = 0, driver/sum.c:631);
+ *   dilate       on the device: the kept cells and their axis neighbours, deduplicated (skip bit AND,
+ *                tier max) and radix-sorted by mixed-radix key, i.e. lexicographically in k
+ *                (driver/sumkey.h:20-90);
  *   levels       sqb_dev_level() for lev = top-1 .. 0 (driver/sum.c:652-799), the cell lists staying
  *                in device memory.
  * Sums of the grow are Neumaier sums in point order as the reference's kadd (driver/sum.c:18-20);
@@ -101,151 +104,62 @@ static int box_zero(Run &R, int lev, long *nev, int *zero){
     return 0;
 }
 
-/* open-addressing set of nonzero 64-bit keys */
-struct KeySet {
-    std::vector<uint64_t> T; uint64_t mask = 0; long n = 0;
-    static uint64_t hh(uint64_t y){ return (y*0x9E3779B97F4A7C15ULL) >> 21; }
-    void init(long cap){ uint64_t c = 1 << 20; while(c < (uint64_t)cap*2) c <<= 1; T.assign(c, 0); mask = c - 1; n = 0; }
-    void grow(){ std::vector<uint64_t> O; O.swap(T); T.assign(O.size()*2, 0); mask = T.size() - 1; n = 0; for(uint64_t y : O) if(y) insert(y); }
-    /* 1 if y was new */
-    int insert(uint64_t y){
-        if((uint64_t)(n + 1)*10 > T.size()*7) grow();
-        uint64_t i = hh(y) & mask;
-        while(T[i]){ if(T[i] == y) return 0; i = (i + 1) & mask; }
-        T[i] = y; n++; return 1;
-    }
-    long find(uint64_t y) const { uint64_t i = hh(y) & mask; while(T[i]){ if(T[i] == y) return (long)i; i = (i + 1) & mask; } return -1; }
-};
-
-/* mixed-radix key (driver/sumkey.h:7-18): 1 c_0 ... c_{D-1} in base W, c_i = k_i/st + K/st; 0 if the
- * keys would not fit 63 bits */
-static int keyradix(const Run &R, int st, uint64_t *P){
+/* mixed-radix key (driver/sumkey.h:7-18): 1 c_0 ... c_{D-1} in base W, c_i = k_i/st + K/st; W = 0 if
+ * the keys would not fit 63 bits; *nbits = bit length of the largest key */
+static int keyradix(const Run &R, int st, uint64_t *P, int *nbits){
     const uint64_t W = 2*(R.K/st) + 1, TOP = 1ULL << 63; uint64_t p = 1;
     for(int i = R.D - 1; i >= 0; i--){ P[i] = p; if(p > TOP/W) return 0; p *= W; }
+    *nbits = 64 - __builtin_clzll(p) + 1;             /* keys < 2 W^D */
     return (int)W;
-}
-static inline uint64_t key_of(const Run &R, const signed char *k, int st, int W){
-    uint64_t y = 1; for(int i = 0; i < R.D; i++) y = y*W + (uint64_t)(k[i]/st + R.K/st); return y;
-}
-static inline void key_pt(const Run &R, uint64_t y, int st, int W, sqb_pt_t *p){
-    memset(p, 0, sizeof *p);
-    for(int i = R.D - 1; i >= 0; i--){ p->k[i] = (signed char)(((int)(y % W) - R.K/st)*st); y /= W; }
 }
 
 struct GrowOut { double S, A, e1, e2, drop, gshs; long gshn, nev; };
 
-/* driver/sumkey.h:126-461 (see the file comment) */
-static int grow(Run &R, int lev, double eps_rel, std::vector<sqb_pt_t> &keep, GrowOut *go){
-    const int st = 1 << lev; uint64_t P[SQB_MAXD]; const int W = keyradix(R, st, P);
+/* driver/sumkey.h:126-461 (see the file comment); the kept cells, dilated at the same step when
+ * dilate_out is given, stay on the device */
+static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated, long *ndil){
+    const int st = 1 << lev; uint64_t P[SQB_MAXD]; int nbits = 0;
+    const int W = keyradix(R, st, P, &nbits);
     if(!W) FAIL("lattice too wide for 64-bit grid keys (D=%d, N=%d, step %dh)", R.D, 2*R.K + 1, st);
     const double pw = pow(st, R.D);
     const int store = lev > 0, gs = lev == 0 && R.o.abskip ? R.o.growskip : 0;
-    KeySet seen; seen.init(1 << 20);
-    std::vector<sqb_pt_t> fr(1), nx; memset(&fr[0], 0, sizeof fr[0]);
-    seen.insert(key_of(R, fr[0].k, st, W));
-    std::vector<double> kv, v; std::vector<unsigned char> nr, sk;
-    ksum ks; double a = 0, x1 = 0, x2 = 0, dr = 0, gshs = 0; long ne = 0, gshn = 0;
-    keep.clear();
-    while(!fr.empty()){
-        const long n = (long)fr.size();
-        sk.assign(n, 0);
-        if(gs) for(long i = 0; i < n; i++) sk[i] = fr[i].k[SQB_PFLAG] > 0;
-        if(eval(R, fr, gs ? sk.data() : NULL, v, nr)) return -1;
+    if(sqb_grow_begin(R.D, R.K, st, W, (const unsigned long long*)P, gs, R.o.abskip, sqb_dev_stream()))
+        FAIL("device grow: %s", sqb_top_error());
+    std::vector<double> v; std::vector<unsigned char> stt, cls;
+    ksum ks; double a = 0, x1 = 0, x2 = 0, dr = 0, gshs = 0; long ne = 0, gshn = 0, nkeep = 0;
+    for(;;){
+        const sqb_pt_t *pts; const unsigned char *skip;
+        const long n = sqb_grow_frontier(&pts, &skip);
+        if(n <= 0) break;
+        v.resize(n); stt.resize(n); cls.resize(n);
+        const double *vd; const unsigned char *sd;
+        if(sqb_dev_eval_resident(R.g, pts, n, skip, &R.t, v.data(), stt.data(), &R.nq, &R.u, &R.unresdrop, &vd, &sd))
+            FAIL("device: %s", sqb_last_error());
+        if(sqb_grow_shells(cls.data())) FAIL("device grow: %s", sqb_top_error());
         ne += n;
+        /* the frontier's sums in point order, then its threshold (driver/sumkey.h:225-245) */
         for(long i = 0; i < n; i++){ ks.add(v[i]*pw); a += fabs(v[i])*pw; }
         const double thr = eps_rel*a;
-        std::vector<long> kj;
         for(long i = 0; i < n; i++){
-            int mx = 0; for(int d = 0; d < R.D; d++){ int x = abs(fr[i].k[d]); if(x > mx) mx = x; }
-            const int kp = fabs(v[i]) >= thr;
             const double w = fabs(v[i])*pw;
-            if(mx == R.K) x1 += w; else if(mx == R.K - st) x2 += w;
-            if(!kp){ dr += w; gshs += v[i]*pw; gshn++; }
-            else {
-                kj.push_back(i); kv.push_back(fabs(v[i]));
-                if(store){ sqb_pt_t p; memset(&p, 0, sizeof p); for(int d = 0; d < R.D; d++) p.k[d] = fr[i].k[d];
-                    if(R.o.abskip) p.k[SQB_PFLAG] = !nr[i];
-                    keep.push_back(p); }
-            }
+            if(cls[i] & 2) x1 += w; else if(cls[i] & 4) x2 += w;
+            if(!(fabs(v[i]) >= thr)){ dr += w; gshs += v[i]*pw; gshn++; }
         }
-        /* the next frontier: unseen axis neighbours of the kept points, first occurrence wins */
-        nx.clear();
-        for(long j : kj){
-            const signed char *k = fr[j].k; const uint64_t y0 = key_of(R, k, st, W);
-            for(int d = 0; d < R.D; d++) for(int sg = -1; sg <= 1; sg += 2){
-                const int kk = k[d] + st*sg; if(kk > R.K || kk < -R.K) continue;
-                const uint64_t y = sg > 0 ? y0 + P[d] : y0 - P[d];
-                if(!seen.insert(y)) continue;
-                sqb_pt_t p; memcpy(&p, &fr[j], sizeof p); p.k[d] = (signed char)kk;
-                if(gs){ const int pg = fr[j].k[SQB_PFLAG]; p.k[SQB_PFLAG] = (signed char)(!sk[j] ? !nr[j] : (pg < gs ? pg + 1 : 0)); }
-                else p.k[SQB_PFLAG] = 0;
-                nx.push_back(p);
-            }
-        }
-        fr.swap(nx);
+        long nk = 0, nn = 0;
+        if(sqb_grow_expand(vd, sd, thr, &nk, &nn)) FAIL("device grow: %s", sqb_top_error());
+        nkeep += nk;
     }
     /* the final threshold, driver/sumkey.h:399-401 */
-    const double thr = eps_rel*a; long m = 0;
-    for(long i = 0; i < (long)kv.size(); i++){
-        if(kv[i] >= thr){ kv[m] = kv[i]; if(store) keep[m] = keep[i]; m++; } else dr += kv[i]*pw;
-    }
-    kv.resize(m); if(store) keep.resize(m);
-    /* shadow tiers by flood fill from z = 0, driver/sumkey.h:402-444 */
-    if(store && m && R.D < SQB_MAXD){
-        KeySet idx; idx.init(m); std::vector<long> hv(idx.T.size(), -1);
-        std::vector<uint64_t> KY(m);
-        for(long i = 0; i < m; i++){ KY[i] = key_of(R, keep[i].k, st, W); }
-        for(long i = 0; i < m; i++){ idx.insert(KY[i]); }
-        hv.assign(idx.T.size(), -1);
-        for(long i = 0; i < m; i++) hv[idx.find(KY[i])] = i;
-        std::vector<unsigned char> tr(m, 0); std::vector<long> cu, nw;
-        for(int t = 1; t <= 2; t++){
-            const double lim = (t == 1 ? 10 : 100)*thr;
-            cu.clear();
-            for(long i = 0; i < m; i++){ int z = 1; for(int d = 0; d < R.D; d++) if(keep[i].k[d]){ z = 0; break; }
-                if(z && kv[i] >= lim){ tr[i] = (unsigned char)t; cu.push_back(i); } }
-            while(!cu.empty()){
-                nw.clear();
-                for(long i : cu) for(int d = 0; d < R.D; d++) for(int sg = -1; sg <= 1; sg += 2){
-                    const int kk = keep[i].k[d] + st*sg; if(kk > R.K || kk < -R.K) continue;
-                    const uint64_t y = sg > 0 ? KY[i] + P[d] : KY[i] - P[d];
-                    const long q = idx.find(y); if(q < 0) continue;
-                    const long j = hv[q];
-                    if(kv[j] >= lim && tr[j] < t){ tr[j] = (unsigned char)t; nw.push_back(j); }
-                }
-                cu.swap(nw);
-            }
-        }
-        for(long i = 0; i < m; i++) keep[i].k[SQB_PFLAG] = (signed char)((keep[i].k[SQB_PFLAG] & 1) | (tr[i] << 1));
-    }
+    const double thr = eps_rel*a;
+    { std::vector<double> kv(nkeep);
+      if(nkeep && sqb_grow_kv(kv.data(), nkeep)) FAIL("device grow: %s", sqb_top_error());
+      for(long i = 0; i < nkeep; i++) if(!(kv[i] >= thr)) dr += kv[i]*pw; }
+    long m = 0;
+    if(sqb_grow_finish(thr, store && R.D < SQB_MAXD, &m)) FAIL("device grow: %s", sqb_top_error());
+    *dilated = NULL; *ndil = 0;
+    if(store && sqb_grow_dilate(nbits, dilated, ndil)) FAIL("device dilate: %s", sqb_top_error());
+    sqb_grow_end();
     go->S = ks.val(); go->A = a; go->e1 = x1; go->e2 = x2; go->drop = dr; go->gshs = gshs; go->gshn = gshn; go->nev = ne;
-    return 0;
-}
-
-/* driver/sumkey.h:20-90: the cells and their axis neighbours at step st, merged flags, key order */
-static int dilate(Run &R, std::vector<sqb_pt_t> &cur, int st){
-    uint64_t P[SQB_MAXD]; const int W = keyradix(R, st, P);
-    if(!W) FAIL("lattice too wide for 64-bit grid keys in dilate");
-    const long n0 = (long)cur.size();
-    if(!n0) return 0;
-    std::vector<std::pair<uint64_t, unsigned char>> c; c.reserve(n0*(2*R.D + 1));
-    for(long q = 0; q < n0; q++){
-        const signed char *k = cur[q].k; const unsigned char fl = (unsigned char)k[SQB_PFLAG];
-        const uint64_t y0 = key_of(R, k, st, W);
-        c.push_back({y0, fl});
-        for(int j = 0; j < R.D; j++) for(int sg = -1; sg <= 1; sg += 2){
-            const int kk = k[j] + st*sg; if(kk > R.K || kk < -R.K) continue;
-            c.push_back({sg > 0 ? y0 + P[j] : y0 - P[j], fl});
-        }
-    }
-    std::sort(c.begin(), c.end(), [](const std::pair<uint64_t, unsigned char> &x, const std::pair<uint64_t, unsigned char> &y){ return x.first < y.first; });
-    cur.clear();
-    for(size_t i = 0; i < c.size();){
-        size_t j = i; int skb = 1, tr = 0;
-        while(j < c.size() && c[j].first == c[i].first){ skb &= c[j].second & 1; int t = c[j].second >> 1; if(t > tr) tr = t; j++; }
-        sqb_pt_t p; key_pt(R, c[i].first, st, W, &p); p.k[SQB_PFLAG] = (signed char)(skb | (tr << 1));
-        cur.push_back(p); i = j;
-    }
     return 0;
 }
 
@@ -270,31 +184,26 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
     }
     if(sqb_dev_tables(R.X.data(), R.Wt.data(), K)) FAIL("device: %s", sqb_last_error());
     const double t0 = now();
+    const unsigned long long l0 = sqb_launch_count() + sqb_top_launches();
+    { double a, b; long c; sqb_kernel_times(&a, &b, &c, 1); }
     set_test(R, R.o.abserr0);
     int zero = 0;
     if(box_zero(R, top, &res->nev, &zero)) return -1;
     if(zero){ res->zero = 1; res->t = now() - t0; return 0; }
-    std::vector<sqb_pt_t> cur; GrowOut go;
-    if(grow(R, top, eps*1e-3, cur, &go)) return -1;
+    GrowOut go; sqb_pt_t *dcur = NULL; long ncur = 0;
+    if(grow(R, top, eps*1e-3, &go, &dcur, &ncur)) return -1;
     res->nev += go.nev; res->ref = go.A; res->prune = go.drop;
     if(top == 0 && go.gshn) res->prune = fabs(go.gshs);
-    if(go.A == 0){ res->t = now() - t0; res->nq = R.nq; return 0; }
+    if(go.A == 0){ sqb_dev_free(dcur); res->t = now() - t0; res->nq = R.nq; res->unresdrop = R.unresdrop; return 0; }
     { double r = go.e2 > 0 ? go.e1/go.e2 : 0; res->trunc = (r > 0 && r < 1) ? go.e1*r/(1 - r) : go.e1; }
     for(int i = 0; i < 3; i++) res->S[i] = NAN;
     double Slev[16]; int nl = 0; Slev[nl++] = go.S;
-    if(top > 0 && dilate(R, cur, 1 << top)) return -1;
-    res->kept_top = (long)cur.size();
+    res->kept_top = ncur;
     res->t_top = now() - t0;
     const int esok = R.D < SQB_MAXD && top > 0;
     /* the levels on the device */
     set_test(R, fmax(R.o.abserr0, R.o.abrel*eps*res->ref));    /* driver/sum.c:651 */
-    sqb_pt_t *dcur = NULL, *dnext = NULL; long ncur = (long)cur.size(), next_cap = 0;
-    if(top > 0){
-        dcur = (sqb_pt_t*)sqb_dev_alloc(ncur*sizeof(sqb_pt_t));
-        if(!dcur) FAIL("device allocation of %ld cells failed", ncur);
-        if(sqb_dev_upload(dcur, cur.data(), ncur*sizeof(sqb_pt_t))){ sqb_dev_free(dcur); FAIL("device: %s", sqb_last_error()); }
-    }
-    std::vector<sqb_pt_t>().swap(cur);
+    sqb_pt_t *dnext = NULL; long next_cap = 0;
     const double tl0 = now(); double es1 = 0, es2 = 0, ah = 0, uu = 0;
     for(int lev = top - 1; lev >= 0; lev--){
         const int st = 1 << lev, last = lev == 0;
@@ -324,10 +233,12 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
     sqb_dev_free(dcur);
     res->t_levels = now() - tl0;
     if(top > 0){ res->unres = sqrt(uu); res->Ah = ah; }
-    else res->unres = sqrt(R.u);
+    else res->unres = R.u;            /* top = 0: the grow's sum of squares as it stands (driver/sum.c:795) */
     res->S[0] = Slev[nl - 1]; res->S[1] = nl > 1 ? Slev[nl - 2] : NAN; res->S[2] = nl > 2 ? Slev[nl - 3] : NAN;
     res->es1 = es1; res->es2 = es2; res->esok = esok;
     res->nq = R.nq; res->unresdrop = R.unresdrop;
+    sqb_kernel_times(&res->f64_ms, &res->dd_ms, &res->f64_launches, 1);
+    res->launches = (long)(sqb_launch_count() + sqb_top_launches() - l0);
     res->t = now() - t0;
     return 0;
 }

@@ -63,6 +63,12 @@ typedef struct {
 
 struct Dev {
     int on, dev, nsm;
+    unsigned long long h2d, d2h;  /* bytes copied by the chosen form's calls */
+    cudaEvent_t t0, t1; void *flush; size_t flushn;
+    unsigned long long launches;   /* kernels of this library launched so far */
+    int ktime;                     /* time the FP64 and dd kernels of the level passes with events */
+    cudaEvent_t k0, k1, d1;
+    double f64_ms, dd_ms; long f64_n;
     char info[256];
     cudaStream_t s;
     cudaEvent_t e0, e1;
@@ -87,6 +93,8 @@ extern "C" int sqb_dev_init(int device){
     snprintf(G.info, sizeof G.info, "%s (sm_%d%d, %d SMs)", p.name, p.major, p.minor, p.multiProcessorCount);
     CKR(cudaStreamCreateWithFlags(&G.s, cudaStreamNonBlocking));
     CKR(cudaEventCreate(&G.e0)); CKR(cudaEventCreate(&G.e1));
+    CKR(cudaEventCreate(&G.k0)); CKR(cudaEventCreate(&G.k1)); CKR(cudaEventCreate(&G.d1));
+    CKR(cudaEventCreate(&G.t0)); CKR(cudaEventCreate(&G.t1));
     CKR(cudaMalloc(&G.acc, sizeof(sqb_acc_t)));
     CKR(cudaMalloc(&G.base, sizeof(unsigned long long)));
     CKR(cudaMalloc(&G.nfb, sizeof(unsigned long long)));
@@ -104,6 +112,7 @@ extern "C" int sqb_dev_tables(const double *X, const double *Wt, int K){
     }
     CKR(cudaMemcpy(G.X, X, nt*sizeof(double), cudaMemcpyHostToDevice));
     CKR(cudaMemcpy(G.Wt, Wt, nt*sizeof(double), cudaMemcpyHostToDevice));
+    G.h2d += 2*nt*sizeof(double);
     G.K = K;
     return 0;
 }
@@ -145,15 +154,25 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
         d.all = 1;
         g->dd(&d, grid_for(g, 1, npts, smem), 128, smem, G.s);
         CKR(cudaGetLastError());
+        G.launches++;
         return 0;
     }
     CKR(cudaMemsetAsync(G.nfb, 0, sizeof(unsigned long long), G.s));
+    if(G.ktime) CKR(cudaEventRecord(G.k0, G.s));
     g->f64(a, grid_for(g, 0, npts, smem), 128, smem, G.s);
     CKR(cudaGetLastError());
+    if(G.ktime) CKR(cudaEventRecord(G.k1, G.s));
     d.list = G.fb; d.nlist = G.nfb; d.listcap = G.cap; d.all = 0;
     /* the queue length is known only on the device: a persistent grid reads it */
     g->dd(&d, grid_for(g, 1, 1L << 30, smem), 128, smem, G.s);
     CKR(cudaGetLastError());
+    G.launches += 2;
+    if(G.ktime){
+        CKR(cudaEventRecord(G.d1, G.s));
+        CKR(cudaEventSynchronize(G.d1));
+        float x = 0, y = 0; cudaEventElapsedTime(&x, G.k0, G.k1); cudaEventElapsedTime(&y, G.k1, G.d1);
+        G.f64_ms += x; G.dd_ms += y; G.f64_n++;
+    }
     return 0;
 }
 
@@ -177,6 +196,7 @@ extern "C" int sqb_dev_eval_nodes(const sqb_graph_t *g, long n, const sqb_pt_t *
         memcpy(G.hpts, pts + i0, m*sizeof(sqb_pt_t));
         CKR(cudaMemcpyAsync(G.dpts, G.hpts, m*sizeof(sqb_pt_t), cudaMemcpyHostToDevice, G.s));
         if(skip){ memcpy(G.hskip, skip + i0, m); CKR(cudaMemcpyAsync(G.dskip, G.hskip, m, cudaMemcpyHostToDevice, G.s)); }
+        G.h2d += m*sizeof(sqb_pt_t) + (skip ? m : 0); G.d2h += m*(2*sizeof(double) + 1);
         sqb_eval_t a; memset(&a, 0, sizeof a); fill_eval(&a, t);
         a.pts = G.dpts; a.n = m; a.esize = 1; a.stride = SQB_MAXD; a.flag_at = -1; a.cells = 0; a.st = 0;
         a.skip = skip ? G.dskip : NULL;
@@ -195,6 +215,50 @@ extern "C" int sqb_dev_eval_nodes(const sqb_graph_t *g, long n, const sqb_pt_t *
     }
     *nq += q; *u += uu; *unres += nd;
     return 0;
+}
+
+/* n device-resident nodes (pt_t, flags ignored; skip per node on the device or NULL): values and status
+ * to the host; the device copies stay valid until the next evaluation (*v_dev, *stt_dev) */
+extern "C" int sqb_dev_eval_resident(const sqb_graph_t *g, const sqb_pt_t *pts, long n, const unsigned char *skip,
+                                     const sqb_test_t *t, double *v, unsigned char *stt, long *nq, double *u, long *unres,
+                                     const double **v_dev, const unsigned char **stt_dev){
+    *v_dev = NULL; *stt_dev = NULL;
+    if(n <= 0) return 0;
+    if(reserve_points(n)) return -1;
+    if(n > G.hcap){
+        if(G.hv){ cudaFreeHost(G.hv); cudaFreeHost(G.hst); cudaFreeHost(G.huu); cudaFreeHost(G.hpts); cudaFreeHost(G.hskip); }
+        long c = 1L << 16; while(c < n) c <<= 1;
+        CKR(cudaMallocHost(&G.hv, c*sizeof(double))); CKR(cudaMallocHost(&G.hst, c)); CKR(cudaMallocHost(&G.huu, c*sizeof(double)));
+        CKR(cudaMallocHost(&G.hpts, c*sizeof(sqb_pt_t))); CKR(cudaMallocHost(&G.hskip, c));
+        G.hcap = c;
+    }
+    sqb_eval_t a; memset(&a, 0, sizeof a); fill_eval(&a, t);
+    a.pts = pts; a.n = n; a.esize = 1; a.stride = SQB_MAXD; a.flag_at = -1; a.cells = 0; a.st = 0; a.skip = skip;
+    if(eval_batch(g, &a, t, n)) return -1;
+    CKR(cudaMemcpyAsync(G.hv, G.v, n*sizeof(double), cudaMemcpyDeviceToHost, G.s));
+    CKR(cudaMemcpyAsync(G.hst, G.stt, n, cudaMemcpyDeviceToHost, G.s));
+    CKR(cudaMemcpyAsync(G.huu, G.uu, n*sizeof(double), cudaMemcpyDeviceToHost, G.s));
+    CKR(cudaStreamSynchronize(G.s));
+    G.d2h += n*(2*sizeof(double) + 1);
+    long q = 0, nd = 0; double uu = 0;
+    memcpy(v, G.hv, n*sizeof(double)); memcpy(stt, G.hst, n);
+    for(long i = 0; i < n; i++){
+        const unsigned char s = G.hst[i];
+        if(s & SQB_FALLBACK){ q++; uu += G.huu[i]; }
+        if(s & SQB_UNRES) nd++;
+    }
+    *nq += q; *u += uu; *unres += nd;
+    *v_dev = G.v; *stt_dev = G.stt;
+    return 0;
+}
+extern "C" void *sqb_dev_stream(void){ return (void*)G.s; }
+/* instrumentation: kernels launched so far; with ktime on, the FP64 and double-double kernels of every
+ * evaluation pass are bracketed by events (one synchronisation per batch) and their times summed */
+extern "C" unsigned long long sqb_launch_count(void){ return G.launches; }
+extern "C" void sqb_kernel_timing(int on){ G.ktime = on; }
+extern "C" void sqb_kernel_times(double *f64_ms, double *dd_ms, long *f64_launches, int reset){
+    *f64_ms = G.f64_ms; *dd_ms = G.dd_ms; *f64_launches = G.f64_n;
+    if(reset){ G.f64_ms = G.dd_ms = 0; G.f64_n = 0; }
 }
 
 /* ---------------------------------------- level reduce ------------------------------------------ */
@@ -365,15 +429,18 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
         CKR(cudaGetLastError());
         sqb_k_finish<<<1, FT, 0, G.s>>>(G.bp, G.bkeep, nb, G.boff, G.acc, G.base);
         CKR(cudaGetLastError());
+        G.launches += 2;
         if(!L->last){
             sqb_k_scatter<<<(unsigned)nb, RT, 0, G.s>>>(r, G.boff, G.base, L->next, L->next_cap, &G.acc->overflow);
             CKR(cudaGetLastError());
+            G.launches++;
         }
     }
     CKR(cudaEventRecord(G.e1, G.s));
     sqb_acc_t h;
     CKR(cudaMemcpyAsync(&h, G.acc, sizeof h, cudaMemcpyDeviceToHost, G.s));
     CKR(cudaStreamSynchronize(G.s));
+    G.d2h += sizeof h;
     float t = 0; cudaEventElapsedTime(&t, G.e0, G.e1); if(ms) *ms = t;
     double *src[6] = {h.S, h.A, h.drop, h.b1, h.b2, h.u}, *dst[6] = {acc->S, acc->A, acc->drop, acc->b1, acc->b2, acc->u};
     for(int q = 0; q < 6; q++){ sqdd x = sqdd(dst[q][0], dst[q][1]) + sqdd(src[q][0], src[q][1]); dst[q][0] = x.hi; dst[q][1] = x.lo; }
@@ -384,8 +451,24 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
 
 extern "C" void *sqb_dev_alloc(size_t bytes){ void *p = NULL; if(cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess){ cudaGetLastError(); return NULL; } return p; }
 extern "C" void sqb_dev_free(void *p){ if(p) cudaFree(p); }
-extern "C" int sqb_dev_upload(void *dst, const void *src, size_t bytes){ CKR(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice)); return 0; }
-extern "C" int sqb_dev_download(void *dst, const void *src, size_t bytes){ CKR(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost)); return 0; }
+extern "C" int sqb_dev_upload(void *dst, const void *src, size_t bytes){ CKR(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice)); G.h2d += bytes; return 0; }
+extern "C" int sqb_dev_download(void *dst, const void *src, size_t bytes){ CKR(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost)); G.d2h += bytes; return 0; }
+extern "C" void sqb_dev_count_copy(unsigned long long h2d, unsigned long long d2h){ G.h2d += h2d; G.d2h += d2h; }
+
+/* measurement helpers: bytes copied between host and device so far; events on the library's stream
+ * around a region of work (device milliseconds); an L2 flush (a memset larger than L2) on that stream */
+extern "C" void sqb_copy_bytes(unsigned long long *h2d, unsigned long long *d2h){ *h2d = G.h2d; *d2h = G.d2h; }
+extern "C" int sqb_timer_start(void){ if(sqb_dev_init(0)) return -1; CKR(cudaEventRecord(G.t0, G.s)); return 0; }
+extern "C" double sqb_timer_stop(void){
+    if(cudaEventRecord(G.t1, G.s) != cudaSuccess || cudaEventSynchronize(G.t1) != cudaSuccess) return -1;
+    float t = 0; cudaEventElapsedTime(&t, G.t0, G.t1); return t;
+}
+extern "C" int sqb_l2_flush(size_t bytes){
+    if(sqb_dev_init(0)) return -1;
+    if(bytes > G.flushn){ if(G.flush) cudaFree(G.flush); G.flush = NULL; CKR(cudaMalloc(&G.flush, bytes)); G.flushn = bytes; }
+    CKR(cudaMemsetAsync(G.flush, G.launches & 255, bytes, G.s));
+    return 0;
+}
 extern "C" size_t sqb_dev_free_bytes(void){ size_t f = 0, t = 0; cudaMemGetInfo(&f, &t); return f; }
 
 /* ------------------------------ plain form: the reference's GPU plug-in ABI ---------------------- */
@@ -526,4 +609,44 @@ extern "C" int sqb_eval_points_impl(const sqb_graph_t *g, long n, const double *
     }
     cudaFree(dsf); cudaFree(dv); cudaFree(dab); cudaFree(dvl); cudaFree(dabl); cudaFree(dsk); cudaFree(dX);
     return 0;
+}
+
+/* FP64 peak probe: independent chains of fused multiply-adds (8 per thread, unrolled) or of adds, on
+ * every SM; flops = 2 per FMA, 1 per add.  The measured rate is the denominator of the evaluation
+ * kernels' roofline (the device has no vendor FP64 figure in this environment). */
+template<int FMA>
+__global__ void __launch_bounds__(256) sqb_k_fp64_probe(double *out, long iters, double a, double b){
+    double x[8];
+#pragma unroll
+    for(int j = 0; j < 8; j++) x[j] = threadIdx.x*1e-9 + j;
+    for(long i = 0; i < iters; i++){
+#pragma unroll
+        for(int j = 0; j < 8; j++) x[j] = FMA ? __fma_rn(x[j], a, b) : __dadd_rn(x[j], b);
+    }
+    double s = 0;
+#pragma unroll
+    for(int j = 0; j < 8; j++) s += x[j];
+    if(s == 1.2345) out[0] = s;      /* keeps the chains alive */
+}
+/* returns the rate in TFLOP/s (fma = 1: FMA, 2 flops each; fma = 0: adds) */
+extern "C" double sqb_probe_fp64(int fma, long iters){
+    if(sqb_dev_init(0)) return -1;
+    double *o; if(cudaMalloc(&o, sizeof(double)) != cudaSuccess) return -1;
+    int per = 0;
+    if(fma) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sqb_k_fp64_probe<1>, 256, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sqb_k_fp64_probe<0>, 256, 0);
+    const int grid = G.nsm*(per > 0 ? per : 4);
+    float best = 1e30f;
+    for(int r = 0; r < 4; r++){
+        cudaEventRecord(G.e0, G.s);
+        if(fma) sqb_k_fp64_probe<1><<<grid, 256, 0, G.s>>>(o, iters, 0.999999, 1e-7);
+        else sqb_k_fp64_probe<0><<<grid, 256, 0, G.s>>>(o, iters, 0.999999, 1e-7);
+        cudaEventRecord(G.e1, G.s);
+        cudaEventSynchronize(G.e1);
+        float t = 0; cudaEventElapsedTime(&t, G.e0, G.e1);
+        if(r && t < best) best = t;
+    }
+    cudaFree(o);
+    const double ops = (double)grid*256*8*(double)iters*(fma ? 2 : 1);
+    return ops/(best*1e-3)/1e12;
 }

@@ -54,6 +54,31 @@ typedef struct {
 } sqb_level_t;
 int  sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n, double *ms);
 
+/* the same for n nodes already on the device (pts, skip device pointers); the values and status come
+ * back to the host (v, stt) and stay on the device until the next evaluation (*v_dev, *stt_dev) */
+int  sqb_dev_eval_resident(const sqb_graph_t *g, const sqb_pt_t *pts, long n, const unsigned char *skip,
+                           const sqb_test_t *t, double *v, unsigned char *stt, long *nq, double *u, long *unres,
+                           const double **v_dev, const unsigned char **stt_dev);
+void *sqb_dev_stream(void);
+
+/* the top level on the device (topgrid.cu): grow frontiers, final threshold, tiers, dilation */
+int  sqb_grow_begin(int D, int K, int st, int W, const unsigned long long *P, int gs, int abskip, void *stream);
+long sqb_grow_frontier(const sqb_pt_t **pts, const unsigned char **skip);
+int  sqb_grow_shells(unsigned char *cls_host);
+int  sqb_grow_expand(const double *v_dev, const unsigned char *stt_dev, double thr, long *nkept, long *nnext);
+int  sqb_grow_kv(double *kv_host, long n);
+int  sqb_grow_finish(double thr, int tiers, long *m);
+int  sqb_grow_dilate(int nbits, sqb_pt_t **out, long *n);
+void sqb_grow_end(void);
+const char *sqb_top_error(void);
+int  sqb_radix_sort_u64(unsigned long long *keys_dev, long n, int nbits, void *stream);
+
+/* instrumentation (runtime.cu, topgrid.cu) */
+unsigned long long sqb_launch_count(void);
+unsigned long long sqb_top_launches(void);
+void sqb_kernel_timing(int on);
+void sqb_kernel_times(double *f64_ms, double *dd_ms, long *f64_launches, int reset);
+
 /* device memory for level lists */
 void *sqb_dev_alloc(size_t bytes);
 void  sqb_dev_free(void *p);

@@ -33,7 +33,8 @@ class Result(C.Structure):
                 ('es1', C.c_double), ('es2', C.c_double), ('esok', C.c_int),
                 ('abskipped', C.c_long), ('unresdrop', C.c_long), ('zero', C.c_int),
                 ('t_top', C.c_double), ('t_levels', C.c_double), ('nlev', C.c_int),
-                ('lev_evals', C.c_long * 16), ('lev_ms', C.c_double * 16)]
+                ('lev_evals', C.c_long * 16), ('lev_ms', C.c_double * 16),
+                ('f64_ms', C.c_double), ('dd_ms', C.c_double), ('f64_launches', C.c_long), ('launches', C.c_long)]
 
 
 class SqbError(RuntimeError):
@@ -62,6 +63,9 @@ def lib():
         L.sqb_eval_points.argtypes = [C.c_char_p, C.c_long, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.sqb_eval_points.restype = C.c_int
         L.sqb_device_info.restype = C.c_char_p
+        L.sqb_kernel_timing.argtypes = [C.c_int]
+        L.sqb_probe_fp64.argtypes = [C.c_int, C.c_long]
+        L.sqb_probe_fp64.restype = C.c_double
         L.gpu_info.restype = C.c_char_p
         _lib = L
     return _lib
@@ -173,3 +177,16 @@ def eval_points(graph, sf, prec=0, ab=1):
 
 def device_info():
     return lib().sqb_device_info().decode()
+
+
+def kernel_timing(on=True):
+    """Bracket the evaluation kernels with events; hsum() results then carry f64_ms and dd_ms."""
+    lib().sqb_kernel_timing(1 if on else 0)
+
+
+def probe_fp64(fma=True, iters=1 << 16):
+    """The device's measured FP64 rate in TFLOP/s (FMA = 2 flops)."""
+    r = lib().sqb_probe_fp64(1 if fma else 0, int(iters))
+    if r < 0:
+        raise SqbError('FP64 probe failed')
+    return r

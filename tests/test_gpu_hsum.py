@@ -60,3 +60,20 @@ def test_all_dd_form_agrees(rows):
     for a, b in zip(rows, dd):
         assert a['evals'] == b['evals'] or abs(a['evals'] - b['evals']) < 1e-3*a['evals']
         assert abs(a['value'] - b['value']) <= 1e-12*abs(b['value']), (a['name'], a['value'], b['value'])
+
+
+THREE_LOOP = ['g3_07', 'g3_17', 'v3_01', 'v3_p4Sm', 'w3_p40c']
+
+
+@pytest.mark.parametrize('name', THREE_LOOP)
+def test_three_loop_graphs_match_the_reference_run(name):
+    """three-loop kernels (D = 4..5) at h = 1.0, N = 97, eps = 1e-12: the reference CPU run (exact build,
+    fold off) on this host, same evaluation count, value within 1e-11 relative"""
+    import refpy
+    if name not in {g['name'] for g in sq.graphs()}:
+        pytest.skip('%s not in this build' % name)
+    rows, _ = refpy.run(refpy.SINCQED_EXACT, 1.0, 97, 1e-12, [name], top=1, env={'SINCQED_SYM': '0'})
+    e = rows[0]
+    r = sq.run(1.0, 97, 1e-12, [name], top=1)[0]
+    assert r['evals'] == e['evals'], (name, r['evals'], e['evals'])
+    assert abs(r['value'] - e['value']) <= 1e-11*abs(e['value']) + 1e-15, (name, r['value'], e['value'])
