@@ -123,6 +123,35 @@ double sqb_timer_stop(void);
 /* overwrite `bytes` of device memory on the library's stream (an L2 flush between timed steps) */
 int  sqb_l2_flush(size_t bytes);
 
+/* ------------------------------------------------------------------------------------------------
+ * 3. One refinement-level batch without allocation.  This entry point has no counterpart in the
+ *    reference: it exists for callers that cannot let the library call cudaMalloc, such as a program
+ *    that owns the device memory through its own pool allocator, or a service whose memory budget is
+ *    fixed when it starts.  It runs the level pass of sqb_hsum (the 2^D children of ncell cells at step
+ *    st: FP64 evaluation, double-double fallback, compensated sums, kept children appended in order) on
+ *    a scratch array built into the library (SQB_NOALLOC_BYTES of device memory per GPU, held until the
+ *    process exits) and calls no cudaMalloc, cudaFree or allocating library routine.
+ *    - cells: device pt_t list (12 bytes per cell: k[0..D-1], flags in byte 11); next: device list for the
+ *      kept children (unused when last != 0), next_cap entries;
+ *    - h, K: the lattice (z = k h, |k| <= K); pw, thr: the level's weight step^D and keep threshold;
+ *      abserr .. dropunres: the per-point test parameters (sqb_opts_t);
+ *    - sums (host, 12 doubles): S, sum|v|, dropped weight, the two shadow-tier sums and the round column,
+ *      each as (hi, lo); counts (host, 6): evaluated, kept, fallback, unresolved, skipped |.| sums,
+ *      kept children that did not fit next_cap;
+ *    - at most SQB_NOALLOC_CHILDREN children (ncell << D) per call, else SQB_NOALLOC_TOO_BIG and nothing
+ *      runs; calls share the scratch, so calls whose GPU work overlaps race: issue them one at a time;
+ *      the first call on a device looks up the scratch address, so make it before any stream capture.
+ *    Returns 0, a negative SQB_NOALLOC_* code or a CUDA error code; sqb_error() has the message. */
+#define SQB_NOALLOC_CHILDREN (1L << 18)
+#define SQB_NOALLOC_BYTES (6700000L)
+#define SQB_NOALLOC_BAD_ARG (-1)
+#define SQB_NOALLOC_TOO_BIG (-2)
+#define SQB_NOALLOC_SETUP (-3)
+int  sqb_level_noalloc(const char *graph, double h, int K, const void *cells, long ncell, int st, int last,
+                       double pw, double thr, double abserr, double nearf, double ddslack,
+                       int abskip, int abcheck, int dropunres, void *next, long next_cap,
+                       double *sums, long long *counts, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -192,6 +192,9 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     tg_o = os.path.join(OBJ, 'topgrid.o')
     if _newer(tg_o, [os.path.join(CSRC, 'topgrid.cu')] + hdrs):
         jobs_list.append([NVCC] + NVFLAGS + ['-c', os.path.join(CSRC, 'topgrid.cu'), '-o', tg_o])
+    na_o = os.path.join(OBJ, 'noalloc.o')
+    if _newer(na_o, [os.path.join(CSRC, 'noalloc.cu')] + hdrs):
+        jobs_list.append([NVCC] + NVFLAGS + ['-c', os.path.join(CSRC, 'noalloc.cu'), '-o', na_o])
     reg_o = os.path.join(OBJ, 'registry.o')
     if _newer(reg_o, [reg] + hdrs):
         jobs_list.append([NVCC] + NVFLAGS + ['-c', reg, '-o', reg_o])
@@ -204,7 +207,7 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     with cf.ThreadPoolExecutor(max_workers=n) as ex:
         for f in [ex.submit(_run, c) for c in jobs_list]:
             f.result()
-    objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, reg_o, eng_o]
+    objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o]
     if _newer(LIBSO, objs):
         _run([NVCC] + ARCH + ['-shared', '-o', LIBSO] + objs + ['-Xcompiler', '-fopenmp', '-lgomp'])
     main_cpp = os.path.join(CSRC, 'main.cpp')

@@ -36,6 +36,7 @@
 
 static char E_[512];
 extern "C" const char *sqb_error(void){ return E_; }
+extern "C" void sqb_set_error_msg(const char *msg){ snprintf(E_, sizeof E_, "%s", msg); }
 #define FAIL(...) do { snprintf(E_, sizeof E_, __VA_ARGS__); return -1; } while(0)
 
 static double now(void){ return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }

@@ -650,3 +650,28 @@ extern "C" double sqb_probe_fp64(int fma, long iters){
     const double ops = (double)grid*256*8*(double)iters*(fma ? 2 : 1);
     return ops/(best*1e-3)/1e12;
 }
+
+/* The reduce / finish / scatter sequence of one level batch on buffers the caller names (used by the
+ * allocation-free entry point, noalloc.cu): v, uu, stt per child; bp, bkeep, boff per tile; acc and
+ * base the accumulator and this batch's first kept slot. */
+extern "C" int sqb_level_tail(const void *cells, long nchildren, int D, int st, int last, int abskip, double pw, double thr,
+                              const double *v, const double *uu, const unsigned char *stt,
+                              void *bp, unsigned *bkeep, unsigned long long *boff, sqb_acc_t *acc, unsigned long long *base,
+                              void *next, long next_cap, void *stream){
+    lvl_t r; r.cells = (const signed char*)cells; r.n = nchildren; r.D = D; r.st = st; r.last = last;
+    r.abskip = abskip; r.pw = pw; r.thr = thr; r.v = v; r.uu = uu; r.stt = stt;
+    const long nb = (nchildren + RTILE - 1)/RTILE;
+    cudaStream_t s = (cudaStream_t)stream;
+    sqb_k_reduce<<<(unsigned)nb, RT, 0, s>>>(r, (part_t*)bp, bkeep);
+    CKR(cudaGetLastError());
+    sqb_k_finish<<<1, FT, 0, s>>>((const part_t*)bp, bkeep, nb, boff, acc, base);
+    CKR(cudaGetLastError());
+    if(!last){
+        sqb_k_scatter<<<(unsigned)nb, RT, 0, s>>>(r, boff, base, (sqb_pt_t*)next, next_cap, &acc->overflow);
+        CKR(cudaGetLastError());
+    }
+    return 0;
+}
+/* bytes of one tile partial (sizing of caller-provided tile buffers) and children per tile */
+extern "C" size_t sqb_level_tile_bytes(void){ return sizeof(part_t); }
+extern "C" long sqb_level_tile_children(void){ return RTILE; }
