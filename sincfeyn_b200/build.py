@@ -139,7 +139,7 @@ def count_flops(graphs):
     exe = os.path.join(BUILD, 'count')
     L = ['/* generated by sincfeyn_b200/build.py: algorithmic flop counter */',
          '#include <stdio.h>', '#include "sqcount.h"', 'long sq_flops;',
-         '#define SQ_TABLE static const', '#define SQ_FUNC', '#define SQ_CHUNK', '#define RABS(x) sq_rabs(x)',
+         '#define SQ_TABLE static const', '#define SQ_FUNC', '#define SQ_CHUNK', '#define SQ_CHUNK_DD', '#define RABS(x) sq_rabs(x)',
          '#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX) \\',
          'static void count_##NAME(void){ sq_count sf[D], ab; for(int d = 0; d < D; d++) sf[d] = sq_count(0.7 + 0.37*d); \\',
          '  sq_flops = 0; sqg_##NAME::K<sq_count, 1>::f_##NAME(sf, &ab); long a1 = sq_flops; \\',

@@ -59,22 +59,26 @@ class KernelSource:
     def chunk(self, fname):
         return re.match(r'(bk|ab)_', fname) is not None
 
-    def body(self):
-        """The QREAL half with each function turned into a static member of the class template."""
+    def body(self, chunk_attr='SQ_CHUNK'):
+        """The QREAL half with each function turned into a static member of the class template; the chunk
+        functions (bk_/ab_) get chunk_attr."""
         def repl(m):
             ret, fname = m.group(1), m.group(2)
-            attr = 'SQ_CHUNK' if self.chunk(fname) else 'SQ_FUNC'
+            attr = chunk_attr if self.chunk(fname) else 'SQ_FUNC'
             return 'static %s %s FN(%s)(' % (attr, ret, fname)
         b = _FDEF.sub(repl, self.qhalf)
-        rest = re.sub(r'static (SQ_CHUNK|SQ_FUNC)', '', b)
+        rest = re.sub(r'static (%s|SQ_FUNC)' % chunk_attr, '', b)
         if re.search(r'\bstatic\b', rest):
             raise ValueError('%s: unexpected static in the QREAL half' % self.path)
         return b
 
 
 def emit(src):
-    """Header text for one graph: namespace sqg_<name> with the tables and the class template, then
-    SQ_GRAPH(...) which the including translation unit defines (kernels, registry entry, or counter)."""
+    """Header text for one graph: namespace sqg_<name> with the tables and two copies of the class
+    template -- K, whose chunk functions are SQ_CHUNK (the FP64 evaluation: inlined, so that their
+    argument arrays stay in registers), and KD, whose chunk functions are SQ_CHUNK_DD (double-double:
+    real calls, which keeps the compile of the large kernels bounded) -- then SQ_GRAPH(...), which the
+    including translation unit defines (kernels and registry entry, or flop counter)."""
     k = KernelSource(src)
     out = ['/* generated by sincfeyn_b200/codegen/kgen.py from %s (QREAL half, arithmetic unchanged) */'
            % re.sub(r'^.*?(kernels/)', r'\1', src),
@@ -83,8 +87,15 @@ def emit(src):
         out.append('SQ_TABLE double %s[%d] = {%s};' % (name, n, vals))
     out += ['#define REAL SqReal_', '#define FN(x) x',
             'template<class SqReal_, int SQ_AB> struct K {',
-            k.body().strip('\n'),
-            '};', '#undef REAL', '#undef FN', '}',
+            k.body('SQ_CHUNK').strip('\n'),
+            '};']
+    if any(k.chunk(f) for _, f in k.funcs):
+        out += ['template<class SqReal_, int SQ_AB> struct KD {',
+                k.body('SQ_CHUNK_DD').strip('\n'),
+                '};']
+    else:
+        out += ['template<class SqReal_, int SQ_AB> using KD = K<SqReal_, SQ_AB>;']
+    out += ['#undef REAL', '#undef FN', '}',
             'SQ_GRAPH(%s, "%s", %d, %d, %d, %d, %d)' % (k.name, k.volkov.replace('"', '\\"'),
                                                         k.L, k.D, k.weight, k.n, k.fixed)]
     return k, '\n'.join(out) + '\n'

@@ -43,9 +43,9 @@ extern "C" const sqb_graph_t *sqb_graph_at(int i){ return i >= 0 && i < SQB_NALL
 
 /* ------------------------------------------------------------------------------------------------ */
 #define RT 256                    /* threads per reduce / scatter CTA */
-#define RPT 8                     /* consecutive children per thread */
+#define RPT 16                    /* consecutive children per thread */
 #define RTILE (RT*RPT)
-#define FT 256                    /* threads of the one-CTA finish kernel */
+#define FT 1024                   /* threads of the one-CTA finish kernel (32 warps) */
 
 typedef struct {
     double S[2], A[2], drop[2], b1[2], b2[2], u[2];
@@ -270,9 +270,13 @@ __device__ __forceinline__ int parent_tier(const lvl_t &a, long i){
     return (a.cells[c*SQB_MAXD + SQB_PFLAG] >> 1) & 3;
 }
 
+/* per tile of RTILE children: S = sum v*pw and the shadow-tier sums in double-double per thread (they
+ * can cancel), sum |v|, the dropped weight and the round column (non-negative) in double per thread,
+ * then double-double across threads in a fixed tree */
 __global__ void __launch_bounds__(RT) sqb_k_reduce(const lvl_t a, part_t *bp, unsigned *bkeep){
     const long t0 = blockIdx.x*(long)RTILE + threadIdx.x*(long)RPT;
-    sqdd S, A, dr, b1, b2, u;
+    sqdd S, b1, b2;
+    double A = 0, dr = 0, uu = 0;
     unsigned ne = 0, nq = 0, nu = 0, nsk = 0, keep = 0;
     for(int j = 0; j < RPT; j++){
         const long i = t0 + j;
@@ -280,90 +284,99 @@ __global__ void __launch_bounds__(RT) sqb_k_reduce(const lvl_t a, part_t *bp, un
         const unsigned char s = a.stt[i];
         if(!(s & SQB_PRESENT)) continue;
         const double v = a.v[i], vp = v*a.pw, av = fabs(v);
-        S = sqdd_add_d(S, vp); A = sqdd_add_d(A, av); ne++;
+        S = sqdd_add_d(S, vp); A += av; ne++;
         nsk += (s & SQB_SKIPPED) ? 1 : 0;
-        if(s & SQB_FALLBACK){ nq++; u = sqdd_add_d(u, a.uu[i]); }
+        if(s & SQB_FALLBACK){ nq++; uu += a.uu[i]; }
         if(s & SQB_UNRES) nu++;
         if(a.last){
             const int te = parent_tier(a, i);
             if(te >= 1) b1 = sqdd_add_d(b1, vp);
             if(te >= 2) b2 = sqdd_add_d(b2, vp);
         } else if(av >= a.thr) keep++;
-        else dr = sqdd_add_d(dr, av*a.pw);
+        else dr += av*a.pw;
     }
+    sqdd Ad(A), dd(dr), ud(uu);
     for(int off = 16; off; off >>= 1){
-        S = S + shfl_dd(S, off); A = A + shfl_dd(A, off); dr = dr + shfl_dd(dr, off);
-        b1 = b1 + shfl_dd(b1, off); b2 = b2 + shfl_dd(b2, off); u = u + shfl_dd(u, off);
+        S = S + shfl_dd(S, off); Ad = Ad + shfl_dd(Ad, off); dd = dd + shfl_dd(dd, off);
+        b1 = b1 + shfl_dd(b1, off); b2 = b2 + shfl_dd(b2, off); ud = ud + shfl_dd(ud, off);
         ne += __shfl_down_sync(0xffffffffu, ne, off); nq += __shfl_down_sync(0xffffffffu, nq, off);
         nu += __shfl_down_sync(0xffffffffu, nu, off); nsk += __shfl_down_sync(0xffffffffu, nsk, off);
         keep += __shfl_down_sync(0xffffffffu, keep, off);
     }
-    __shared__ part_t wp[RT/32];
-    __shared__ unsigned wk[RT/32];
+    __shared__ double wd[RT/32][12];
+    __shared__ unsigned wc[RT/32][5];
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     if(l == 0){
-        part_t p; p.S[0] = S.hi; p.S[1] = S.lo; p.A[0] = A.hi; p.A[1] = A.lo; p.drop[0] = dr.hi; p.drop[1] = dr.lo;
-        p.b1[0] = b1.hi; p.b1[1] = b1.lo; p.b2[0] = b2.hi; p.b2[1] = b2.lo; p.u[0] = u.hi; p.u[1] = u.lo;
-        p.ne = ne; p.nq = nq; p.unres = nu; p.skipped = nsk;
-        wp[w] = p; wk[w] = keep;
+        wd[w][0] = S.hi; wd[w][1] = S.lo; wd[w][2] = Ad.hi; wd[w][3] = Ad.lo; wd[w][4] = dd.hi; wd[w][5] = dd.lo;
+        wd[w][6] = b1.hi; wd[w][7] = b1.lo; wd[w][8] = b2.hi; wd[w][9] = b2.lo; wd[w][10] = ud.hi; wd[w][11] = ud.lo;
+        wc[w][0] = ne; wc[w][1] = nq; wc[w][2] = nu; wc[w][3] = nsk; wc[w][4] = keep;
     }
     __syncthreads();
-    if(threadIdx.x == 0){
-        part_t r = wp[0]; unsigned k = wk[0];
-        for(int j = 1; j < RT/32; j++){
-            const part_t &p = wp[j];
-#define ADDP(F) { sqdd x = sqdd(r.F[0], r.F[1]) + sqdd(p.F[0], p.F[1]); r.F[0] = x.hi; r.F[1] = x.lo; }
-            ADDP(S) ADDP(A) ADDP(drop) ADDP(b1) ADDP(b2) ADDP(u)
-            r.ne += p.ne; r.nq += p.nq; r.unres += p.unres; r.skipped += p.skipped; k += wk[j];
+    if(w == 0){
+        const int nw = RT/32;
+        sqdd x[6]; unsigned c[5];
+        for(int q = 0; q < 6; q++) x[q] = l < nw ? sqdd(wd[l][2*q], wd[l][2*q + 1]) : sqdd(0.0);
+        for(int q = 0; q < 5; q++) c[q] = l < nw ? wc[l][q] : 0;
+        for(int off = nw/2; off; off >>= 1){
+            for(int q = 0; q < 6; q++) x[q] = x[q] + shfl_dd(x[q], off);
+            for(int q = 0; q < 5; q++) c[q] += __shfl_down_sync(0xffffffffu, c[q], off);
         }
-        bp[blockIdx.x] = r; bkeep[blockIdx.x] = k;
+        if(l == 0){
+            part_t p;
+            p.S[0] = x[0].hi; p.S[1] = x[0].lo; p.A[0] = x[1].hi; p.A[1] = x[1].lo; p.drop[0] = x[2].hi; p.drop[1] = x[2].lo;
+            p.b1[0] = x[3].hi; p.b1[1] = x[3].lo; p.b2[0] = x[4].hi; p.b2[1] = x[4].lo; p.u[0] = x[5].hi; p.u[1] = x[5].lo;
+            p.ne = c[0]; p.nq = c[1]; p.unres = c[2]; p.skipped = c[3];
+            bp[blockIdx.x] = p; bkeep[blockIdx.x] = c[4];
+        }
     }
 }
 
 /* one CTA: the tiles' offsets (exclusive scan of their kept counts) and the batch's sums, in a fixed
- * order, added into the level accumulator; *base = this batch's first slot in the next list */
+ * order (each thread a contiguous run of tiles, then a fixed tree), added into the level accumulator;
+ * *base = this batch's first slot in the next list */
 __global__ void __launch_bounds__(FT) sqb_k_finish(const part_t *bp, const unsigned *bkeep, long nb,
                                                    unsigned long long *boff, sqb_acc_t *acc, unsigned long long *base){
-    __shared__ double sh[FT][12];
-    __shared__ unsigned long long sc[FT][5];
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, w = t >> 5, l = t & 31;
     const long ch = (nb + FT - 1)/FT, j0 = t*ch, j1 = j0 + ch < nb ? j0 + ch : nb;
-    sqdd S, A, dr, b1, b2, u; unsigned long long ne = 0, nq = 0, nu = 0, nsk = 0, kp = 0;
+    sqdd x[6]; unsigned long long c[5] = {0, 0, 0, 0, 0};
     for(long j = j0; j < j1; j++){
         const part_t &p = bp[j];
-        S = S + sqdd(p.S[0], p.S[1]); A = A + sqdd(p.A[0], p.A[1]); dr = dr + sqdd(p.drop[0], p.drop[1]);
-        b1 = b1 + sqdd(p.b1[0], p.b1[1]); b2 = b2 + sqdd(p.b2[0], p.b2[1]); u = u + sqdd(p.u[0], p.u[1]);
-        ne += p.ne; nq += p.nq; nu += p.unres; nsk += p.skipped; kp += bkeep[j];
+        x[0] = x[0] + sqdd(p.S[0], p.S[1]); x[1] = x[1] + sqdd(p.A[0], p.A[1]); x[2] = x[2] + sqdd(p.drop[0], p.drop[1]);
+        x[3] = x[3] + sqdd(p.b1[0], p.b1[1]); x[4] = x[4] + sqdd(p.b2[0], p.b2[1]); x[5] = x[5] + sqdd(p.u[0], p.u[1]);
+        c[0] += p.ne; c[1] += p.nq; c[2] += p.unres; c[3] += p.skipped; c[4] += bkeep[j];
     }
-    sh[t][0] = S.hi; sh[t][1] = S.lo; sh[t][2] = A.hi; sh[t][3] = A.lo; sh[t][4] = dr.hi; sh[t][5] = dr.lo;
-    sh[t][6] = b1.hi; sh[t][7] = b1.lo; sh[t][8] = b2.hi; sh[t][9] = b2.lo; sh[t][10] = u.hi; sh[t][11] = u.lo;
-    sc[t][0] = ne; sc[t][1] = nq; sc[t][2] = nu; sc[t][3] = nsk; sc[t][4] = kp;
-    __syncthreads();
-    /* exclusive scan of the per-thread kept counts (thread 0, FT values), then per-tile offsets */
-    __shared__ unsigned long long pre[FT];
-    if(t == 0){ unsigned long long x = 0; for(int j = 0; j < FT; j++){ pre[j] = x; x += sc[j][4]; } }
-    __syncthreads();
-    { unsigned long long x = pre[t]; for(long j = j0; j < j1; j++){ boff[j] = x; x += bkeep[j]; } }
-    /* fixed-order tree of the sums */
-    for(int h = FT/2; h; h >>= 1){
-        if(t < h){
-            for(int q = 0; q < 12; q += 2){
-                sqdd x = sqdd(sh[t][q], sh[t][q + 1]) + sqdd(sh[t + h][q], sh[t + h][q + 1]);
-                sh[t][q] = x.hi; sh[t][q + 1] = x.lo;
-            }
-            for(int q = 0; q < 4; q++) sc[t][q] += sc[t + h][q];
-        }
-        __syncthreads();
+    /* exclusive scan of the kept counts: warp scan, then across warps */
+    __shared__ unsigned long long wsum[FT/32], wpre[FT/32];
+    unsigned long long inc = c[4];
+    for(int off = 1; off < 32; off <<= 1){ unsigned long long y = __shfl_up_sync(0xffffffffu, inc, off); if(l >= off) inc += y; }
+    if(l == 31) wsum[w] = inc;
+    /* the sums: warp tree, then the warps' results */
+    for(int off = 16; off; off >>= 1){
+        for(int q = 0; q < 6; q++) x[q] = x[q] + shfl_dd(x[q], off);
+        for(int q = 0; q < 4; q++) c[q] += __shfl_down_sync(0xffffffffu, c[q], off);
     }
-    if(t == 0){
-        unsigned long long total = pre[FT - 1] + sc[FT - 1][4];
-        double *dst[6] = {acc->S, acc->A, acc->drop, acc->b1, acc->b2, acc->u};
-        for(int q = 0; q < 6; q++){
-            sqdd x = sqdd(dst[q][0], dst[q][1]) + sqdd(sh[0][2*q], sh[0][2*q + 1]);
-            dst[q][0] = x.hi; dst[q][1] = x.lo;
+    __shared__ double wd[FT/32][12];
+    __shared__ unsigned long long wc[FT/32][4];
+    if(l == 0){ for(int q = 0; q < 6; q++){ wd[w][2*q] = x[q].hi; wd[w][2*q + 1] = x[q].lo; } for(int q = 0; q < 4; q++) wc[w][q] = c[q]; }
+    __syncthreads();
+    if(t == 0){ unsigned long long s = 0; for(int q = 0; q < FT/32; q++){ wpre[q] = s; s += wsum[q]; } }
+    __syncthreads();
+    { unsigned long long o = wpre[w] + inc - c[4]; for(long j = j0; j < j1; j++){ boff[j] = o; o += bkeep[j]; } }
+    if(w == 0){
+        sqdd y[6]; unsigned long long d[4];
+        for(int q = 0; q < 6; q++) y[q] = sqdd(wd[l][2*q], wd[l][2*q + 1]);
+        for(int q = 0; q < 4; q++) d[q] = wc[l][q];
+        for(int off = 16; off; off >>= 1){
+            for(int q = 0; q < 6; q++) y[q] = y[q] + shfl_dd(y[q], off);
+            for(int q = 0; q < 4; q++) d[q] += __shfl_down_sync(0xffffffffu, d[q], off);
         }
-        acc->ne += sc[0][0]; acc->nq += sc[0][1]; acc->unres += sc[0][2]; acc->skipped += sc[0][3];
-        *base = acc->keep; acc->keep += total;
+        if(l == 0){
+            const unsigned long long total = wpre[FT/32 - 1] + wsum[FT/32 - 1];
+            double *dst[6] = {acc->S, acc->A, acc->drop, acc->b1, acc->b2, acc->u};
+            for(int q = 0; q < 6; q++){ sqdd z = sqdd(dst[q][0], dst[q][1]) + y[q]; dst[q][0] = z.hi; dst[q][1] = z.lo; }
+            acc->ne += d[0]; acc->nq += d[1]; acc->unres += d[2]; acc->skipped += d[3];
+            *base = acc->keep; acc->keep += total;
+        }
     }
 }
 

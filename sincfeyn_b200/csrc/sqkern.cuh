@@ -22,7 +22,8 @@
 
 #define SQ_TABLE static __constant__ const
 #define SQ_FUNC __device__
-#define SQ_CHUNK __device__ __noinline__
+#define SQ_CHUNK __device__ __forceinline__      /* FP64: chunk arguments stay in registers */
+#define SQ_CHUNK_DD __device__ __noinline__     /* double-double: real calls bound the compile */
 #define RABS(x) sq_rabs(x)
 
 #ifndef SQB_BLOCK
@@ -161,6 +162,8 @@ struct F {                                                                      
     template<class R, int AB> static __device__ __forceinline__ R f(const R *sf, R *ab){           \
         return K<R, AB>::f_##NAME(sf, ab); }                                                       \
 };                                                                                                 \
+template<> __device__ __forceinline__ sqdd F::f<sqdd, 1>(const sqdd *sf, sqdd *ab){                \
+    return KD<sqdd, 1>::f_##NAME(sf, ab); }                                                        \
 static void f64(const sqb_eval_t *a, int grid, int block, size_t smem, void *st){                  \
     sqb_k_f64<F, D><<<grid, block, smem, (cudaStream_t)st>>>(*a); }                                \
 static void dd(const sqb_dd_t *a, int grid, int block, size_t smem, void *st){                     \

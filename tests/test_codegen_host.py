@@ -27,6 +27,7 @@ SRC = r'''
 #define SQ_TABLE static const
 #define SQ_FUNC
 #define SQ_CHUNK
+#define SQ_CHUNK_DD
 #define RABS(x) sq_rabs(x)
 #define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
 extern "C" int hg_##NAME(long n, const double *sf, int prec, int ab, double *f, double *a){       \
