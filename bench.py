@@ -184,6 +184,12 @@ def main():
     L.sqb_timer_stop.restype = C.c_double
     L.sqb_l2_flush.argtypes = [C.c_size_t]
     sq.kernel_timing(True)
+    # the device code of every graph of the set is loaded before the timed region (CUDA loads a kernel
+    # on its first launch otherwise); the one-time cost is reported as load_s
+    t_load = time.perf_counter()
+    for g in names:
+        sq.preload(g)
+    t_load = time.perf_counter() - t_load
     # warm-up: the first W integrals of the set, untimed
     for g in names[:args.warmup]:
         sq.hsum(g, H, N_PTS, EPS, device=local)
@@ -213,7 +219,8 @@ def main():
         launches += r['launches'] + 1
         a1, a0 = flops[g]
         fl += (r['nev'] - r['abskipped'])*a1 + r['abskipped']*a0
-        results.append([g, r['S'][0]*weight[g], r['nev'], r['nq'], round(ms, 2)])
+        results.append([g, r['S'][0]*weight[g], r['nev'], r['nq'], round(ms, 2), round(1e3*r['t_top'], 2),
+                        round(sum(r['lev_ms']), 2)])
     torch.cuda.synchronize()
     wall = time.perf_counter() - t_wall
     clk = clocks.stop()
@@ -244,6 +251,7 @@ def main():
         'config': {'workload': '%s (%d integrals) h=%g N=%d eps=%g top=2, FP64 + double-double fallback'
                                % (SET, len(names), H, N_PTS, EPS),
                    'integrals_timed': args.steps, 'l2': 'flushed (256 MiB memset) before every step',
+                   'kernels': 'device code of the set\'s kernels loaded before the timed region (load_s %.2f s, once per process)' % t_load,
                    'parallelism': 'integrals dealt round-robin over %d GPU(s)' % world},
         'time_to_sum_s': step_ms*1e-3 if args.steps >= len(names) else None,
         'e2e': {'value': nev/(step_ms*1e-3), 'unit': 'points/s', 'h2d_bytes_per_step': int(h2d/args.steps),
@@ -254,6 +262,7 @@ def main():
                      'peak_source': 'measured FP64 FMA rate (probe kernel, this device)',
                      'flops_per_launch': fl/max(1, f64_n), 'launches': int(f64_n)},
         'gpu_launches': int(launches),
+        'load_s': t_load,
         'clocks': clk,
         'points': int(nev), 'level_points': int(lev_ev),
     }
@@ -271,7 +280,7 @@ def main():
             L.sqb_timer_start(); sq.hsum(g, H, N_PTS, EPS); t_f += L.sqb_timer_stop()
             L.sqb_timer_start(); sq.hsum(g, H, N_PTS, EPS, alldd=1); t_d += L.sqb_timer_stop()
         line['vs_alldd'] = {'sample': ALLDD_SAMPLE, 'fp64dd_s': t_f*1e-3, 'alldd_s': t_d*1e-3, 'speedup': t_d/t_f}
-    line['per_integral'] = {'columns': ['graph', 'value', 'evals', 'fallback', 'ms'], 'rows': results}
+    line['per_integral'] = {'columns': ['graph', 'value', 'evals', 'fallback', 'ms', 'top_ms', 'levels_ms'], 'rows': results}
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -108,6 +108,10 @@ int  sqb_eval_points(const char *graph, long n, const double *sf, int prec, int 
 
 /* the device the library runs on ("off" before the first call) */
 const char *sqb_device_info(void);
+/* load the device code of a graph's kernels now (graph NULL: all graphs); CUDA otherwise loads each
+ * kernel on its first launch, up to about a second for the largest graphs.  Returns the number of
+ * kernels loaded, or -1 */
+int  sqb_preload(const char *graph);
 
 /* instrumentation: bracket every FP64 and double-double evaluation launch with events (one
  * synchronisation per batch) so that sqb_result_t carries their times; and the measured FP64 rate of

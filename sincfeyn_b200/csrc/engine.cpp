@@ -213,7 +213,7 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
         L.pw = pow(st, R.D); L.thr = eps*res->ref*1e-2; L.t = R.t; L.max_children = R.o.max_children;
         if(!last){
             double want = (double)ncur*(double)(1L << R.D);
-            double room = 0.45*(double)sqb_dev_free_bytes()/sizeof(sqb_pt_t);
+            double room = 0.35*(double)sqb_dev_total_bytes()/sizeof(sqb_pt_t);
             next_cap = (long)(want < room ? want : room) + 1;
             dnext = (sqb_pt_t*)sqb_dev_alloc(next_cap*sizeof(sqb_pt_t));
             if(!dnext){ sqb_dev_free(dcur); FAIL("device allocation of the next level (%ld cells) failed", next_cap); }

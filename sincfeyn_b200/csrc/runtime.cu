@@ -92,6 +92,10 @@ extern "C" int sqb_dev_init(int device){
     G.dev = device; G.nsm = p.multiProcessorCount;
     snprintf(G.info, sizeof G.info, "%s (sm_%d%d, %d SMs)", p.name, p.major, p.minor, p.multiProcessorCount);
     CKR(cudaStreamCreateWithFlags(&G.s, cudaStreamNonBlocking));
+    /* the cell lists and the grow's tables come from the device's stream-ordered pool, which keeps
+     * freed memory for the next integral instead of returning it (no cudaFree synchronisation) */
+    { cudaMemPool_t pool; CKR(cudaDeviceGetDefaultMemPool(&pool, device));
+      unsigned long long keep = ~0ULL; CKR(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)); }
     CKR(cudaEventCreate(&G.e0)); CKR(cudaEventCreate(&G.e1));
     CKR(cudaEventCreate(&G.k0)); CKR(cudaEventCreate(&G.k1)); CKR(cudaEventCreate(&G.d1));
     CKR(cudaEventCreate(&G.t0)); CKR(cudaEventCreate(&G.t1));
@@ -252,6 +256,22 @@ extern "C" int sqb_dev_eval_resident(const sqb_graph_t *g, const sqb_pt_t *pts, 
     return 0;
 }
 extern "C" void *sqb_dev_stream(void){ return (void*)G.s; }
+
+/* Load the device code of a graph's kernels now (NULL: every graph).  CUDA loads a kernel's code on
+ * its first launch by default (lazy loading); for this library's large per-graph kernels that first
+ * launch costs up to a second, so a caller that times integrals, or wants the cost at start-up,
+ * preloads.  Returns the number of kernels loaded, or -1. */
+extern "C" int sqb_preload(const char *graph){
+    if(sqb_dev_init(0)) return -1;
+    int n = 0;
+    for(int i = 0; i < SQB_NALL; i++){
+        const sqb_graph_t *g = SQB_ALL[i];
+        if(graph && strcmp(graph, g->name)) continue;
+        sqb_kattr_t at;
+        for(int which = 0; which < 2; which++) if(g->attr(which, 128, 4096, &at)) n++;
+    }
+    return n;
+}
 /* instrumentation: kernels launched so far; with ktime on, the FP64 and double-double kernels of every
  * evaluation pass are bracketed by events (one synchronisation per batch) and their times summed */
 extern "C" unsigned long long sqb_launch_count(void){ return G.launches; }
@@ -462,8 +482,8 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
     return 0;
 }
 
-extern "C" void *sqb_dev_alloc(size_t bytes){ void *p = NULL; if(cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess){ cudaGetLastError(); return NULL; } return p; }
-extern "C" void sqb_dev_free(void *p){ if(p) cudaFree(p); }
+extern "C" void *sqb_dev_alloc(size_t bytes){ void *p = NULL; if(cudaMallocAsync(&p, bytes ? bytes : 16, G.s) != cudaSuccess){ cudaGetLastError(); return NULL; } return p; }
+extern "C" void sqb_dev_free(void *p){ if(p) cudaFreeAsync(p, G.s); }
 extern "C" int sqb_dev_upload(void *dst, const void *src, size_t bytes){ CKR(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice)); G.h2d += bytes; return 0; }
 extern "C" int sqb_dev_download(void *dst, const void *src, size_t bytes){ CKR(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost)); G.d2h += bytes; return 0; }
 extern "C" void sqb_dev_count_copy(unsigned long long h2d, unsigned long long d2h){ G.h2d += h2d; G.d2h += d2h; }
@@ -483,6 +503,7 @@ extern "C" int sqb_l2_flush(size_t bytes){
     return 0;
 }
 extern "C" size_t sqb_dev_free_bytes(void){ size_t f = 0, t = 0; cudaMemGetInfo(&f, &t); return f; }
+extern "C" size_t sqb_dev_total_bytes(void){ size_t f = 0, t = 0; cudaMemGetInfo(&f, &t); return t; }
 
 /* ------------------------------ plain form: the reference's GPU plug-in ABI ---------------------- */
 /* Same contract as driver/gpu.cu:1-103: two slots, each with its own stream, event and pinned buffers;

@@ -85,6 +85,7 @@ void  sqb_dev_free(void *p);
 int   sqb_dev_upload(void *dst, const void *src, size_t bytes);
 int   sqb_dev_download(void *dst, const void *src, size_t bytes);
 size_t sqb_dev_free_bytes(void);
+size_t sqb_dev_total_bytes(void);
 
 #ifdef __cplusplus
 }

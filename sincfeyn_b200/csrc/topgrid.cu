@@ -114,6 +114,10 @@ __global__ void __launch_bounds__(TG_T) k_scatter(Op op, long n, const unsigned 
 struct Scratch { unsigned *bcnt; unsigned long long *boff, *tot; long nbcap; };
 static Scratch SC;
 static cudaStream_t TS;
+/* stream-ordered allocation from the device's memory pool: no device-wide synchronisation, and the pool
+ * keeps freed memory for the next integral (the runtime sets its release threshold) */
+#define DMALLOC(p, n) cudaMallocAsync((void**)(p), (n), TS)
+#define DFREE(p) cudaFreeAsync((p), TS)
 static unsigned long long TL;    /* kernels launched by this file */
 extern "C" unsigned long long sqb_top_launches(void){ return TL; }
 extern "C" void sqb_dev_count_copy(unsigned long long h2d, unsigned long long d2h);
@@ -121,10 +125,10 @@ extern "C" void sqb_dev_count_copy(unsigned long long h2d, unsigned long long d2
 static int scratch(long n){
     long nb = (n + TG_TILE - 1)/TG_TILE; if(nb < 1) nb = 1;
     if(nb <= SC.nbcap) return 0;
-    if(SC.bcnt){ cudaFree(SC.bcnt); cudaFree(SC.boff); }
+    if(SC.bcnt){ DFREE(SC.bcnt); DFREE(SC.boff); }
     long c = 1024; while(c < nb) c <<= 1;
-    TCK(cudaMalloc(&SC.bcnt, c*sizeof(unsigned))); TCK(cudaMalloc(&SC.boff, c*sizeof(unsigned long long)));
-    if(!SC.tot) TCK(cudaMalloc(&SC.tot, sizeof(unsigned long long)));
+    TCK(DMALLOC(&SC.bcnt, c*sizeof(unsigned))); TCK(DMALLOC(&SC.boff, c*sizeof(unsigned long long)));
+    if(!SC.tot) TCK(DMALLOC(&SC.tot, sizeof(unsigned long long)));
     SC.nbcap = c;
     return 0;
 }
@@ -176,12 +180,12 @@ static int table_room(long extra){
     if((double)(GR.nseen + extra) <= 0.6*cap) return 0;
     long nc = cap; while((double)(GR.nseen + extra) > 0.6*nc) nc <<= 1;
     unsigned long long *k2; unsigned *w2;
-    TCK(cudaMalloc(&k2, nc*sizeof(unsigned long long))); TCK(cudaMalloc(&w2, nc*sizeof(unsigned)));
+    TCK(DMALLOC(&k2, nc*sizeof(unsigned long long))); TCK(DMALLOC(&w2, nc*sizeof(unsigned)));
     TCK(cudaMemsetAsync(k2, 0, nc*sizeof(unsigned long long), TS)); TCK(cudaMemsetAsync(w2, 0, nc*sizeof(unsigned), TS));
     k_rehash<<<1184, 256, 0, TS>>>(GR.key, GR.word, cap, k2, w2, (unsigned long long)(nc - 1), GR.err); TL++;
     TCK(cudaGetLastError());
     TCK(cudaStreamSynchronize(TS));
-    cudaFree(GR.key); cudaFree(GR.word);
+    DFREE(GR.key); DFREE(GR.word);
     GR.key = k2; GR.word = w2; GR.mask = (unsigned long long)(nc - 1);
     return 0;
 }
@@ -189,9 +193,9 @@ static int table_room(long extra){
 template<class T> static int devbuf(T **p, long *cap, long n, long keep){
     if(n <= *cap && *p) return 0;
     long c = 1L << 16; while(c < n) c <<= 1;
-    T *q; TCK(cudaMalloc(&q, c*sizeof(T)));
+    T *q; TCK(DMALLOC(&q, c*sizeof(T)));
     if(*p && keep > 0){ TCK(cudaMemcpyAsync(q, *p, keep*sizeof(T), cudaMemcpyDeviceToDevice, TS)); TCK(cudaStreamSynchronize(TS)); }
-    if(*p) cudaFree(*p);
+    if(*p) DFREE(*p);
     *p = q; *cap = c;
     return 0;
 }
@@ -200,13 +204,13 @@ static int frontier_room(long n){
     if(n <= GR.frcap && GR.fr) return 0;
     long c = 1L << 16; while(c < n) c <<= 1;
     sqb_pt_t *a, *b; unsigned char *s1, *s2, *s3;
-    TCK(cudaMalloc(&a, c*sizeof(sqb_pt_t))); TCK(cudaMalloc(&b, c*sizeof(sqb_pt_t)));
-    TCK(cudaMalloc(&s1, c)); TCK(cudaMalloc(&s2, c)); TCK(cudaMalloc(&s3, c));
+    TCK(DMALLOC(&a, c*sizeof(sqb_pt_t))); TCK(DMALLOC(&b, c*sizeof(sqb_pt_t)));
+    TCK(DMALLOC(&s1, c)); TCK(DMALLOC(&s2, c)); TCK(DMALLOC(&s3, c));
     if(GR.fr){
         TCK(cudaMemcpyAsync(a, GR.fr, GR.nfr*sizeof(sqb_pt_t), cudaMemcpyDeviceToDevice, TS));
         TCK(cudaMemcpyAsync(s1, GR.frsk, GR.nfr, cudaMemcpyDeviceToDevice, TS));
         TCK(cudaStreamSynchronize(TS));
-        cudaFree(GR.fr); cudaFree(GR.nx); cudaFree(GR.frsk); cudaFree(GR.nxsk); cudaFree(GR.cls);
+        DFREE(GR.fr); DFREE(GR.nx); DFREE(GR.frsk); DFREE(GR.nxsk); DFREE(GR.cls);
     }
     GR.fr = a; GR.nx = b; GR.frsk = s1; GR.nxsk = s2; GR.cls = s3; GR.frcap = c;
     return 0;
@@ -228,11 +232,11 @@ extern "C" int sqb_grow_begin(int D, int K, int st, int W, const unsigned long l
     GR.g.D = D; GR.g.K = K; GR.g.st = st; GR.g.W = W; for(int i = 0; i < D; i++) GR.g.P[i] = P[i];
     GR.gs = gs; GR.abskip = abskip; GR.nseen = 1; GR.nkeep = 0; GR.nfr = 0;
     const long cap = 1L << 22;
-    if(GR.key){ cudaFree(GR.key); cudaFree(GR.word); GR.key = NULL; }
-    TCK(cudaMalloc(&GR.key, cap*sizeof(unsigned long long))); TCK(cudaMalloc(&GR.word, cap*sizeof(unsigned)));
+    if(GR.key){ DFREE(GR.key); DFREE(GR.word); GR.key = NULL; }
+    TCK(DMALLOC(&GR.key, cap*sizeof(unsigned long long))); TCK(DMALLOC(&GR.word, cap*sizeof(unsigned)));
     TCK(cudaMemsetAsync(GR.key, 0, cap*sizeof(unsigned long long), TS)); TCK(cudaMemsetAsync(GR.word, 0, cap*sizeof(unsigned), TS));
     GR.mask = (unsigned long long)(cap - 1);
-    if(!GR.err) TCK(cudaMalloc(&GR.err, sizeof(unsigned long long)));
+    if(!GR.err) TCK(DMALLOC(&GR.err, sizeof(unsigned long long)));
     TCK(cudaMemsetAsync(GR.err, 0, sizeof(unsigned long long), TS));
     if(frontier_room(1)) return -1;
     unsigned long long y0 = 1; for(int i = 0; i < D; i++) y0 = y0*W + (unsigned long long)(K/st);
@@ -397,18 +401,18 @@ __global__ void k_tier_apply(sqb_pt_t *keep, const unsigned *tr, long m){
 /* the final threshold and the tiers; *m = kept points left; the keep list stays on the device */
 extern "C" int sqb_grow_finish(double thr, int tiers, long *m_out){
     sqb_pt_t *out; double *okv; const long n = GR.nkeep;
-    TCK(cudaMalloc(&out, (n ? n : 1)*sizeof(sqb_pt_t))); TCK(cudaMalloc(&okv, (n ? n : 1)*sizeof(double)));
+    TCK(DMALLOC(&out, (n ? n : 1)*sizeof(sqb_pt_t))); TCK(DMALLOC(&okv, (n ? n : 1)*sizeof(double)));
     RethOp ro; ro.keep = GR.keep; ro.kv = GR.kv; ro.thr = thr; ro.out = out; ro.okv = okv;
     long m = 0;
     if(compact(ro, n, &m)) return -1;
-    cudaFree(GR.keep); cudaFree(GR.kv); GR.keep = out; GR.kv = okv; GR.keepcap = n ? n : 1; GR.nkeep = m;
+    DFREE(GR.keep); DFREE(GR.kv); GR.keep = out; GR.kv = okv; GR.keepcap = n ? n : 1; GR.nkeep = m;
     *m_out = m;
     if(!tiers || !m) return 0;
     long cap = 1L << 20; while(cap < 2*m) cap <<= 1;
     unsigned long long *key; unsigned *word, *tr; long *cu, *nw; unsigned long long *cnt;
-    TCK(cudaMalloc(&key, cap*sizeof(unsigned long long))); TCK(cudaMalloc(&word, cap*sizeof(unsigned)));
-    TCK(cudaMalloc(&tr, m*sizeof(unsigned))); TCK(cudaMalloc(&cu, m*sizeof(long))); TCK(cudaMalloc(&nw, m*sizeof(long)));
-    TCK(cudaMalloc(&cnt, 2*sizeof(unsigned long long)));
+    TCK(DMALLOC(&key, cap*sizeof(unsigned long long))); TCK(DMALLOC(&word, cap*sizeof(unsigned)));
+    TCK(DMALLOC(&tr, m*sizeof(unsigned))); TCK(DMALLOC(&cu, m*sizeof(long))); TCK(DMALLOC(&nw, m*sizeof(long)));
+    TCK(DMALLOC(&cnt, 2*sizeof(unsigned long long)));
     TCK(cudaMemsetAsync(key, 0, cap*sizeof(unsigned long long), TS)); TCK(cudaMemsetAsync(tr, 0, m*sizeof(unsigned), TS));
     k_index<<<1184, 256, 0, TS>>>(GR.g, GR.keep, m, key, word, (unsigned long long)(cap - 1), GR.err); TL++;
     for(int t = 1; t <= 2; t++){
@@ -427,7 +431,7 @@ extern "C" int sqb_grow_finish(double thr, int tiers, long *m_out){
     k_tier_apply<<<1184, 256, 0, TS>>>(GR.keep, tr, m); TL++;
     TCK(cudaGetLastError());
     TCK(cudaStreamSynchronize(TS));
-    cudaFree(key); cudaFree(word); cudaFree(tr); cudaFree(cu); cudaFree(nw); cudaFree(cnt);
+    DFREE(key); DFREE(word); DFREE(tr); DFREE(cu); DFREE(nw); DFREE(cnt);
     return 0;
 }
 
@@ -513,8 +517,8 @@ static int radix_sort(unsigned long long **a, unsigned long long **b, long n, in
     if(n <= 1) return 0;
     const long nblk = (n + RS_TILE - 1)/RS_TILE;
     unsigned *hist; unsigned long long *off, *tot;
-    TCK(cudaMalloc(&hist, 256*nblk*sizeof(unsigned))); TCK(cudaMalloc(&off, 256*nblk*sizeof(unsigned long long)));
-    TCK(cudaMalloc(&tot, sizeof(unsigned long long)));
+    TCK(DMALLOC(&hist, 256*nblk*sizeof(unsigned))); TCK(DMALLOC(&off, 256*nblk*sizeof(unsigned long long)));
+    TCK(DMALLOC(&tot, sizeof(unsigned long long)));
     for(int sh = 0; sh < nbits; sh += 8){
         k_rs_hist<<<(unsigned)nblk, RS_T, 0, TS>>>(*a, n, sh, hist, nblk); TL++;
         k_scan<<<1, 256, 0, TS>>>(hist, 256*nblk, off, tot); TL++;
@@ -523,16 +527,16 @@ static int radix_sort(unsigned long long **a, unsigned long long **b, long n, in
         unsigned long long *t = *a; *a = *b; *b = t;
     }
     TCK(cudaStreamSynchronize(TS));
-    cudaFree(hist); cudaFree(off); cudaFree(tot);
+    DFREE(hist); DFREE(off); DFREE(tot);
     return 0;
 }
 extern "C" int sqb_radix_sort_u64(unsigned long long *keys_dev, long n, int nbits, void *stream){
     TS = (cudaStream_t)stream;
     unsigned long long *b, *a = keys_dev;
-    TCK(cudaMalloc(&b, (n ? n : 1)*sizeof(unsigned long long)));
+    TCK(DMALLOC(&b, (n ? n : 1)*sizeof(unsigned long long)));
     if(radix_sort(&a, &b, n, nbits)) return -1;
-    if(a != keys_dev){ TCK(cudaMemcpy(keys_dev, a, n*sizeof(unsigned long long), cudaMemcpyDeviceToDevice)); cudaFree(a); }
-    else cudaFree(b);
+    if(a != keys_dev){ TCK(cudaMemcpy(keys_dev, a, n*sizeof(unsigned long long), cudaMemcpyDeviceToDevice)); DFREE(a); }
+    else DFREE(b);
     return 0;
 }
 
@@ -545,8 +549,8 @@ extern "C" int sqb_grow_dilate(int nbits, sqb_pt_t **out, long *n){
     long cap = 1L << 20; while(cap < 4*n0) cap <<= 1;
     for(;;){
         unsigned long long *key, *cnt; unsigned *skb, *trm;
-        TCK(cudaMalloc(&key, cap*sizeof(unsigned long long))); TCK(cudaMalloc(&skb, cap*sizeof(unsigned)));
-        TCK(cudaMalloc(&trm, cap*sizeof(unsigned))); TCK(cudaMalloc(&cnt, sizeof(unsigned long long)));
+        TCK(DMALLOC(&key, cap*sizeof(unsigned long long))); TCK(DMALLOC(&skb, cap*sizeof(unsigned)));
+        TCK(DMALLOC(&trm, cap*sizeof(unsigned))); TCK(DMALLOC(&cnt, sizeof(unsigned long long)));
         TCK(cudaMemsetAsync(key, 0, cap*sizeof(unsigned long long), TS)); TCK(cudaMemsetAsync(skb, 0xff, cap*sizeof(unsigned), TS));
         TCK(cudaMemsetAsync(trm, 0, cap*sizeof(unsigned), TS)); TCK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), TS));
         TCK(cudaMemsetAsync(GR.err, 0, sizeof(unsigned long long), TS));
@@ -556,17 +560,17 @@ extern "C" int sqb_grow_dilate(int nbits, sqb_pt_t **out, long *n){
         TCK(cudaMemcpyAsync(&m, cnt, sizeof m, cudaMemcpyDeviceToHost, TS));
         TCK(cudaMemcpyAsync(&e, GR.err, sizeof e, cudaMemcpyDeviceToHost, TS));
         TCK(cudaStreamSynchronize(TS));
-        if(e || (double)m > 0.75*cap){ cudaFree(key); cudaFree(skb); cudaFree(trm); cudaFree(cnt); cap *= 2; continue; }
+        if(e || (double)m > 0.75*cap){ DFREE(key); DFREE(skb); DFREE(trm); DFREE(cnt); cap *= 2; continue; }
         unsigned long long *U, *T;
-        TCK(cudaMalloc(&U, m*sizeof(unsigned long long))); TCK(cudaMalloc(&T, m*sizeof(unsigned long long)));
+        TCK(DMALLOC(&U, m*sizeof(unsigned long long))); TCK(DMALLOC(&T, m*sizeof(unsigned long long)));
         SlotOp so; so.key = key; so.out = U; long mm = 0;
         if(compact(so, cap, &mm)) return -1;
         if(radix_sort(&U, &T, mm, nbits)) return -1;
-        sqb_pt_t *o; TCK(cudaMalloc(&o, mm*sizeof(sqb_pt_t)));
+        sqb_pt_t *o; TCK(DMALLOC(&o, mm*sizeof(sqb_pt_t)));
         k_dil_decode<<<1184, 256, 0, TS>>>(GR.g, U, mm, key, skb, trm, (unsigned long long)(cap - 1), o); TL++;
         TCK(cudaGetLastError());
         TCK(cudaStreamSynchronize(TS));
-        cudaFree(U); cudaFree(T); cudaFree(key); cudaFree(skb); cudaFree(trm); cudaFree(cnt);
+        DFREE(U); DFREE(T); DFREE(key); DFREE(skb); DFREE(trm); DFREE(cnt);
         *out = o; *n = mm;
         return 0;
     }
@@ -574,8 +578,8 @@ extern "C" int sqb_grow_dilate(int nbits, sqb_pt_t **out, long *n){
 
 /* top = 0 keeps no list; the kept list is released with the table */
 extern "C" void sqb_grow_end(void){
-    if(GR.key){ cudaFree(GR.key); cudaFree(GR.word); GR.key = NULL; }
-    if(GR.keep){ cudaFree(GR.keep); GR.keep = NULL; GR.keepcap = 0; }
-    if(GR.kv){ cudaFree(GR.kv); GR.kv = NULL; }
+    if(GR.key){ DFREE(GR.key); DFREE(GR.word); GR.key = NULL; }
+    if(GR.keep){ DFREE(GR.keep); GR.keep = NULL; GR.keepcap = 0; }
+    if(GR.kv){ DFREE(GR.kv); GR.kv = NULL; }
     GR.nkeep = 0;
 }

@@ -179,6 +179,16 @@ def device_info():
     return lib().sqb_device_info().decode()
 
 
+def preload(graph=None):
+    """Load the device code of a graph's kernels (None: all graphs) before timing or at start-up."""
+    L = lib()
+    L.sqb_preload.argtypes = [C.c_char_p]
+    n = L.sqb_preload(graph.encode() if graph else None)
+    if n < 0:
+        raise SqbError('preload failed')
+    return n
+
+
 def kernel_timing(on=True):
     """Bracket the evaluation kernels with events; hsum() results then carry f64_ms and dd_ms."""
     lib().sqb_kernel_timing(1 if on else 0)
