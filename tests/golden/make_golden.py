@@ -12,7 +12,7 @@ Fixtures
   boxsum_gl.json                the reference's pointwise known-answer program
                                 (mathematica/check/boxsum_gl.c): term values at k = 0 and k = (1,-1,2,0),
                                 h = 1, and full-box sums at h = 1, K = 6, for the five two-loop kernels
-  pointwise_<class>.npz         400 (g3: 128) seeded nodes per graph, sigma = e^z, z ~ U[-3,3] (the protocol of
+  pointwise_<class>.npz         400 (g3: 128, v4/w4: 32) seeded nodes per graph, sigma = e^z, z ~ U[-3,3] (the protocol of
                                 tests/check_onept.sh): fd with SQ_AB = 1 and 0 and fq (hi, lo) of the
                                 reference kernels
 """
@@ -31,12 +31,20 @@ import refpy  # noqa: E402
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
+def with_log(rows, out):
+    """add the log line's fallback count and kept top-level cells (driver/main.c:58-65) to the rows"""
+    for r in rows:
+        m = re.search(r'^%s .* evals (\d+) quad (\d+) kept (\d+)' % re.escape(r['name']), out, re.M)
+        r['quad'], r['kept_top'] = int(m.group(2)), int(m.group(3))
+    return rows
+
+
 def all2():
     d = {'command': 'run 1.0 97 1e-12 all2'}
-    rows, _ = refpy.run(refpy.SINCQED, 1.0, 97, 1e-12, ['all2'])
-    d['reference'] = rows
-    rows, _ = refpy.run(refpy.SINCQED_EXACT, 1.0, 97, 1e-12, ['all2'], env={'SINCQED_SYM': '0'})
-    d['reference_exact_unfolded'] = rows
+    rows, out = refpy.run(refpy.SINCQED, 1.0, 97, 1e-12, ['all2'])
+    d['reference'] = with_log(rows, out)
+    rows, out = refpy.run(refpy.SINCQED_EXACT, 1.0, 97, 1e-12, ['all2'], env={'SINCQED_SYM': '0'})
+    d['reference_exact_unfolded'] = with_log(rows, out)
     for r in d['reference'] + d['reference_exact_unfolded']:
         r.pop('time_s', None)
     with open(os.path.join(OUT, 'all2_h1.0_N97_eps1e-12.json'), 'w') as f:
@@ -82,3 +90,5 @@ if __name__ == '__main__':
     pointwise('g2', ('g2_', 'v2_'))
     pointwise('v3', ('v3_', 'w3_'))
     pointwise('g3', ('g3_',), 128)
+    pointwise('v4', ('v4_',), 32)
+    pointwise('w4', ('w4_',), 32)

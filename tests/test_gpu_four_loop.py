@@ -1,0 +1,25 @@
+"""Four-loop lepton-loop kernels (kernels/v4, kernels/w4) through the chosen form (GPU), against the
+reference CPU run on this host (exact build, fold off) at h = 1.0, N = 97, eps = 1e-12: same evaluation
+count, values within the four-loop tolerance 1e-11 relative; and v4_00 against the exactly known
+lepton-loop value I(a) = 0.000876865858890 (docs/LEPTON_LOOPS.md:5-17) to the accuracy h = 1.0 gives."""
+import pytest
+
+import refpy
+from sincfeyn_b200 import sq
+
+pytestmark = pytest.mark.gpu
+
+GRAPHS = ['v4_00', 'w4_00Sc', 'v4_40', 'w4_01Sc']
+
+
+@pytest.mark.parametrize('name', GRAPHS)
+def test_four_loop_graph_matches_the_reference_run(name):
+    if name not in {g['name'] for g in sq.graphs()}:
+        pytest.skip('%s not in this build' % name)
+    rows, _ = refpy.run(refpy.SINCQED_EXACT, 1.0, 97, 1e-12, [name], top=1, env={'SINCQED_SYM': '0'})
+    e = rows[0]
+    r = sq.run(1.0, 97, 1e-12, [name], top=1)[0]
+    assert r['evals'] == e['evals'], (name, r['evals'], e['evals'])
+    assert abs(r['value'] - e['value']) <= 1e-11*abs(e['value']) + 1e-18, (name, r['value'], e['value'])
+    if name == 'v4_00':
+        assert abs(r['value'] - 0.000876865858890) < 1e-6

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 NOT_BITWISE = {'g3_lbl'}
 
 
-@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3'])
+@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3', 'v4', 'w4'])
 def test_fp64_and_dd_bitwise(cls):
     z = np.load(os.path.join(GOLD, 'pointwise_%s.npz' % cls))
     have = {g['name'] for g in sq.graphs()}
