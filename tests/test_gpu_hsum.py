@@ -72,7 +72,7 @@ def test_three_loop_graphs_match_the_reference_run(name):
     import refpy
     if name not in {g['name'] for g in sq.graphs()}:
         pytest.skip('%s not in this build' % name)
-    rows, _ = refpy.run(refpy.SINCQED_EXACT, 1.0, 97, 1e-12, [name], top=1, env={'SINCQED_SYM': '0'})
+    rows, _ = refpy.run(refpy.SINCQED_EXACT, 1.0, 97, 1e-12, [name], top=1, env={'SINCQED_SYM': '0', 'SINCQED_KEEPBT': '1'})
     e = rows[0]
     r = sq.run(1.0, 97, 1e-12, [name], top=1)[0]
     assert r['evals'] == e['evals'], (name, r['evals'], e['evals'])
