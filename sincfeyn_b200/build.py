@@ -63,12 +63,18 @@ def _run(cmd, log=None):
     return r.stdout
 
 
+SYNTH = os.path.join(PKG, 'synth')
+
+
 def kernel_sources(kdir, classes):
+    """the reference's kernels of these classes, then the synthetic integrands of sincfeyn_b200/synth"""
     out = []
     for c in classes.split():
         d = os.path.join(kdir, c)
         if os.path.isdir(d):
             out += sorted(os.path.join(d, f) for f in os.listdir(d) if f.endswith('.c'))
+    if out:
+        out += sorted(os.path.join(SYNTH, f) for f in os.listdir(SYNTH) if f.endswith('.c'))
     return out
 
 
@@ -140,6 +146,7 @@ def count_flops(graphs):
     L = ['/* generated by sincfeyn_b200/build.py: algorithmic flop counter */',
          '#include <stdio.h>', '#include "sqcount.h"', 'long sq_flops;',
          '#define SQ_TABLE static const', '#define SQ_FUNC', '#define SQ_CHUNK', '#define SQ_CHUNK_DD', '#define RABS(x) sq_rabs(x)',
+         '#define SQ_EXP(x) sq_exp(x)', '#define SQ_LOG(x) sq_log(x)',
          '#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX) \\',
          'static void count_##NAME(void){ sq_count sf[D], ab; for(int d = 0; d < D; d++) sf[d] = sq_count(0.7 + 0.37*d); \\',
          '  sq_flops = 0; sqg_##NAME::K<sq_count, 1>::f_##NAME(sf, &ab); long a1 = sq_flops; \\',

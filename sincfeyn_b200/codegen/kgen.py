@@ -28,6 +28,7 @@ import sys
 
 _DESC = re.compile(r'^const graph_t G_(\w+)=\{"([^"]*)","([^"]*)",(\d+),(\d+),(\d+),(\d+),(\d+),', re.M)
 _GL = re.compile(r'^static const double (GL[XW]_\w+)\[(\d+)\]=\{([^}]*)\}(?:, (GL[XW]_\w+)\[(\d+)\]=\{([^}]*)\})?;', re.M)
+_TAB1 = re.compile(r'^static const double (\w+)\[(\d+)\]=\{([^}]*)\};$', re.M)
 _FDEF = re.compile(r'^static (REAL|void) FN\((\w+)\)\(', re.M)
 
 
@@ -48,6 +49,9 @@ class KernelSource:
             self.gl.append((g.group(1), int(g.group(2)), g.group(3)))
             if g.group(4):
                 self.gl.append((g.group(4), int(g.group(5)), g.group(6)))
+        for g in _TAB1.finditer(txt):                 # single-table lines (the synthetic integrands)
+            if g.group(1) not in [t[0] for t in self.gl]:
+                self.gl.append((g.group(1), int(g.group(2)), g.group(3)))
         i = txt.index('#define REAL QREAL')
         j = txt.index('#define FN(x) x##_q', i) + len('#define FN(x) x##_q')
         k = txt.index('#undef REAL', j)

@@ -42,6 +42,7 @@ static int selected(const char *name, const char *volkov, int L, const char *s){
     if(!strcmp(s, "lbl4")) return !strncmp(name, "l4_", 3);
     if(!strcmp(s, "pi6"))  return !strncmp(name, "w4_p6", 5);
     if(!strcmp(s, "lbl"))  return !strcmp(name, "g3_lbl");
+    if(!strcmp(s, "synth")) return !strncmp(name, "syn_", 4);   /* the seeded synthetic integrands (no graph) */
     return 0;
 }
 static int isnum(const char *s){ char *e; strtod(s, &e); return e != s && *e == 0; }

@@ -131,3 +131,50 @@ SQDD_HD sqdd sq_rabs(const sqdd &x){ return x < sqdd(0.0) ? -x : x; }
 /* in double the sign of a zero never reaches a result (every |.| value is only added and multiplied
  * into non-negative sums), so the single sign-clearing instruction is used */
 SQDD_HD double sq_rabs(double x){ return fabs(x); }
+
+/* e^a in double-double, by the method of argument reduction and repeated squaring published for
+ * double-double arithmetic by Hida, Li and Bailey (2001): a = m ln2 + r with m = rint(a/ln2), r scaled
+ * by 2^-10 (|r| <= 3.4e-4), e^r - 1 by its Taylor series to degree 9 in Horner form (truncation below
+ * 1e-33 relative), ten doublings e^{2x} - 1 = (e^x - 1)(e^x + 1), then (1 + s) 2^m.  ln 2 is a
+ * triple-double and 1/n! double-double roundings of 300-bit values.  Relative error about 1e-32 for
+ * |a| <= 700 while the result's low part stays normal (|a| <= ~670).  Every step is a double-double operation of this file,
+ * so host and device results agree bit for bit. */
+SQDD_HD sqdd sqdd_exp(const sqdd &a){
+    if(a.hi > 709.0) return sqdd(exp(a.hi));          /* overflow: +inf */
+    if(a.hi < -745.0) return sqdd(0.0);
+    const sqdd LN2(6.9314718055994529e-01, 2.3190468138462996e-17);
+    const double LN2C = 5.7077084384162121e-34;        /* third term of ln 2: r stays accurate for |m| ~ 1000 */
+    const double m = rint(SQ_DIV(a.hi, LN2.hi));
+    sqdd r = a - LN2*m;
+    r = sqdd_add_d(r, -SQ_MUL(LN2C, m));
+    r = sqdd(SQ_MUL(r.hi, 0x1p-10), SQ_MUL(r.lo, 0x1p-10));
+    const sqdd C[7] = {
+    /* 1/9! */ sqdd(2.7557319223985893e-06, -1.8583932740464721e-22),
+    /* 1/8! */ sqdd(2.4801587301587302e-05, 2.1511947866775882e-23),
+    /* 1/7! */ sqdd(0.00019841269841269841, 1.7209558293420705e-22),
+    /* 1/6! */ sqdd(0.0013888888888888889, -5.3005439543735771e-20),
+    /* 1/5! */ sqdd(0.0083333333333333332, 1.1564823173178714e-19),
+    /* 1/4! */ sqdd(0.041666666666666664, 2.3129646346357427e-18),
+    /* 1/3! */ sqdd(0.16666666666666666, 9.2518585385429707e-18),
+    };
+    sqdd s = C[0];
+    for(int i = 1; i < 7; i++) s = s*r + C[i];
+    s = s*r + 0.5;
+    s = s*r + 1.0;
+    s = s*r;
+    for(int i = 0; i < 10; i++) s = s*(s + 2.0);
+    s = s + 1.0;
+    return sqdd(ldexp(s.hi, (int)m), ldexp(s.lo, (int)m));
+}
+/* log a in double-double: one Newton step x + a e^{-x} - 1 from the double logarithm of the high part */
+SQDD_HD sqdd sqdd_log(const sqdd &a){
+    if(!(a.hi > 0)) return sqdd(log(a.hi));
+    const sqdd x(log(a.hi));
+    return x + a*sqdd_exp(-x) - 1;
+}
+/* exp and log for the integrands that need them (SQ_EXP, SQ_LOG): the double versions are the math
+ * library's, the double-double versions the ones above */
+SQDD_HD double sq_exp(double x){ return exp(x); }
+SQDD_HD double sq_log(double x){ return log(x); }
+SQDD_HD sqdd sq_exp(const sqdd &x){ return sqdd_exp(x); }
+SQDD_HD sqdd sq_log(const sqdd &x){ return sqdd_log(x); }

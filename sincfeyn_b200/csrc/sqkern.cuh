@@ -25,6 +25,8 @@
 #define SQ_CHUNK __device__ __forceinline__      /* FP64: chunk arguments stay in registers */
 #define SQ_CHUNK_DD __device__ __noinline__     /* double-double: real calls bound the compile */
 #define RABS(x) sq_rabs(x)
+#define SQ_EXP(x) sq_exp(x)
+#define SQ_LOG(x) sq_log(x)
 
 #ifndef SQB_BLOCK
 #define SQB_BLOCK 128

@@ -129,7 +129,8 @@ def select(selectors):
             return True
         return {'all2': g['L'] == 2, 'all3': g['L'] == 3 and not n.startswith('w3_'), 'all4': g['L'] == 4,
                 'q3': n.startswith('g3_') and n != 'g3_lbl', 'vp3': n.startswith('v3_'),
-                'vp4': n.startswith('v4_') or n.startswith('w4_'), 'lbl': n == 'g3_lbl'}.get(s, False)
+                'vp4': n.startswith('v4_') or n.startswith('w4_'), 'lbl': n == 'g3_lbl',
+                'synth': n.startswith('syn_')}.get(s, False)
     out = []
     for s in selectors:
         for g in gs:

@@ -15,6 +15,14 @@ Fixtures
   pointwise_<class>.npz         400 (g3: 128, v4/w4: 32) seeded nodes per graph, sigma = e^z, z ~ U[-3,3] (the protocol of
                                 tests/check_onept.sh): fd with SQ_AB = 1 and 0 and fq (hi, lo) of the
                                 reference kernels
+  pointwise_synth.npz           the same for the synthetic integrands syn_d5, syn_d8, syn_d11 (64 nodes each),
+                                evaluated by the oracle build (the synthetic sources compiled with the
+                                reference's double-double type and oracle/sqsynth.h)
+  synth_runs.json               the reference's hsum() on the synthetic integrands, -ffp-contract=off build,
+                                SINCQED_SYM=0 and SINCQED_KEEPBT=1 (one boundary table, the exact grow):
+                                syn_d5 at h = 1.0 (N = 61) and h = 0.7 (N = 87), syn_d8 at h = 1.0 (N = 61)
+
+    python tests/golden/make_golden.py [all2 boxsum pointwise synth]   # default: all of them
 """
 import json
 import os
@@ -84,11 +92,33 @@ def pointwise(cls, prefixes, npts=400):
     np.savez_compressed(os.path.join(OUT, 'pointwise_%s.npz' % cls), **arrays)
 
 
+SYNTH_RUNS = [('syn_d5', 1.0, 61), ('syn_d5', 0.7, 87), ('syn_d8', 1.0, 61)]
+
+
+def synth():
+    pointwise('synth', ('syn_',), 64)
+    d = {'env': {'SINCQED_SYM': '0', 'SINCQED_KEEPBT': '1'}, 'eps': 1e-12, 'runs': []}
+    for name, h, N in SYNTH_RUNS:
+        rows, out = refpy.run(refpy.SINCQED_EXACT, h, N, 1e-12, [name], env=d['env'])
+        r = with_log(rows, out)[0]
+        r.pop('time_s', None)
+        r.update(h=h, N=N)
+        d['runs'].append(r)
+    with open(os.path.join(OUT, 'synth_runs.json'), 'w') as f:
+        json.dump(d, f, indent=1)
+
+
 if __name__ == '__main__':
-    all2()
-    boxsum()
-    pointwise('g2', ('g2_', 'v2_'))
-    pointwise('v3', ('v3_', 'w3_'))
-    pointwise('g3', ('g3_',), 128)
-    pointwise('v4', ('v4_',), 32)
-    pointwise('w4', ('w4_',), 32)
+    parts = sys.argv[1:] or ['all2', 'boxsum', 'pointwise', 'synth']
+    if 'all2' in parts:
+        all2()
+    if 'boxsum' in parts:
+        boxsum()
+    if 'pointwise' in parts:
+        pointwise('g2', ('g2_', 'v2_'))
+        pointwise('v3', ('v3_', 'w3_'))
+        pointwise('g3', ('g3_',), 128)
+        pointwise('v4', ('v4_',), 32)
+        pointwise('w4', ('w4_',), 32)
+    if 'synth' in parts:
+        synth()
