@@ -147,6 +147,126 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+MIX_H = (1.0, 0.9, 0.8, 0.7)
+MIX_SETS = ('all2', 'all3')
+
+
+def mixed_jobs(sq):
+    """The mixed batch: every two- and three-loop integral at h = 1.0, 0.9, 0.8, 0.7, N = 2 ceil(48/h) + 1,
+    eps = 1e-12 (184 integrals of D = 3..7); cost estimate (2/h)^D for the largest-first order."""
+    info = {g['name']: g for g in sq.graphs()}
+    jobs = []
+    for h in MIX_H:
+        N = 2*math.ceil(48/h - 1e-9) + 1
+        for g in sq.select(list(MIX_SETS)):
+            jobs.append((g, h, N, EPS, -1, (2.0/h)**info[g]['D']))
+    return jobs
+
+
+def run_mixed(args, sq, L):
+    """--workload mixed: the batch one integral at a time (one worker) against the tuned concurrent
+    batch (sqb_hsum_batch); device time of each whole batch, points/s, and the two runs' values, which
+    must be identical (each integral's arithmetic does not depend on the schedule)."""
+    import torch
+    jobs = mixed_jobs(sq)
+    for g in sorted({j[0] for j in jobs}):
+        sq.preload(g)
+    sample = jobs[::8]
+    # warm-up: the calibration sample once per candidate is the tuner's own run
+    best, rates = sq.batch_tune(sample, (1, 2, 4, 6, 8))
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    seq, ms_seq = sq.hsum_batch(jobs, workers=1)
+    bat, ms_bat = sq.hsum_batch(jobs, workers=best)
+    clk = clocks.stop()
+    nev = sum(r['nev'] for r in seq)
+    same = all(all(x == y or (x != x and y != y) for x, y in zip(a['S'], b['S'])) and a['nev'] == b['nev']
+               for a, b in zip(seq, bat))
+    info = {g['name']: g for g in sq.graphs()}
+    per_h = {}
+    for j, r in zip(jobs, bat):
+        per_h.setdefault(j[1], [0.0, 0])
+        per_h[j[1]][0] += r['S'][0]*info[j[0]]['weight']
+        per_h[j[1]][1] += r['nev']
+    line = {'workload': 'mixed', 'metric': 'integrand points/s of the mixed batch (all2+all3 x h=1.0,0.9,0.8,0.7)',
+            'value': nev/(ms_bat*1e-3), 'unit': 'points/s', 'n_gpus': 1, 'higher_is_better': True,
+            'integrals': len(jobs), 'points': nev,
+            'batched': {'workers': best, 'device_s': ms_bat*1e-3, 'points_s': nev/(ms_bat*1e-3)},
+            'one_at_a_time': {'workers': 1, 'device_s': ms_seq*1e-3, 'points_s': nev/(ms_seq*1e-3)},
+            'speedup': ms_seq/ms_bat, 'identical_results': same,
+            'tuner': {'sample': '%d integrals (every 8th)' % len(sample), 'points_s_by_workers': rates, 'chosen': best},
+            'sums_by_h': {str(h): {'sum': v[0], 'points': v[1]} for h, v in sorted(per_h.items())},
+            'clocks': clk, 'dtype': 'f64+dd', 'data': 'the reference kernels (kernels/g2, g3, v3)',
+            'config': {'workload': 'all2+all3 at h in %s, N=2ceil(48/h)+1, eps=%g, default top' % (list(MIX_H), EPS)}}
+    print(json.dumps(line), flush=True)
+
+
+SYN_D = (5, 8, 11)
+SYN_H = (1.0, 0.7)
+GOLDEN_SYNTH = os.path.join(ROOT, 'tests', 'golden', 'synth_runs.json')
+FLOPS_JSON = os.path.join(ROOT, 'sincfeyn_b200', 'lib', 'flops.json')
+
+
+def run_synth(args, sq, L):
+    """--workload synth: the synthetic Sinc-sum microbenchmark (d = 5, 8, 11; h = 1.0, 0.7; N =
+    2 ceil(30/h) + 1; eps = 1e-12).  Per case: points/s and FP64 rate of the FP64+dd form, and the
+    precision table: the value in FP64 only (no fallback: the fallback bound set to infinity), FP64+dd,
+    all double-double (d <= 8), against the reference's hsum() on the host-double-double oracle build
+    where a golden run exists (d = 5 both h, d = 8 at h = 1.0)."""
+    import torch
+    with open(FLOPS_JSON) as f:
+        fl = json.load(f)
+    gold = {}
+    if os.path.exists(GOLDEN_SYNTH):
+        with open(GOLDEN_SYNTH) as f:
+            for r in json.load(f)['runs']:
+                gold[(r['name'], r['h'])] = r['value']
+    peak = sq.probe_fp64(True)
+    for d in SYN_D:
+        sq.preload('syn_d%d' % d)
+    # warm-up: the smallest case in every form (device buffers, pinned staging)
+    for kw in ({}, {'abserr0': 1e300}, {'alldd': 1}):
+        sq.run(1.0, 61, EPS, ['syn_d5'], **kw)
+    rows = []
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    for d in SYN_D:
+        name = 'syn_d%d' % d
+        for h in SYN_H:
+            N = 2*math.ceil(30/h - 1e-9) + 1
+            row = {'d': d, 'h': h, 'N': N}
+            for form, kw in (('fp64dd', {}), ('fp64', {'abserr0': 1e300}), ('alldd', {'alldd': 1})):
+                if form == 'alldd' and d > 8:
+                    continue
+                L.sqb_timer_start()
+                r = sq.run(h, N, EPS, [name], **kw)[0]
+                ms = L.sqb_timer_stop()
+                raw = r['raw']
+                row[form] = {'value': r['value'], 'evals': r['evals'], 'fallback': r['quad'], 'device_s': ms*1e-3,
+                             'points_s': r['evals']/(ms*1e-3)}
+                if form == 'fp64dd':
+                    a1, a0, tr = fl[name]['ab1'], fl[name]['ab0'], fl[name].get('tr', 0)
+                    fk = (r['evals'] - raw['abskipped'])*a1 + raw['abskipped']*a0
+                    row['fp64_kernel'] = {'ms': raw['f64_ms'], 'flops_per_point': a1, 'exp_log_per_point': tr,
+                                          'arith_tflops': fk/(raw['f64_ms']*1e-3)/1e12 if raw['f64_ms'] else None,
+                                          'exp_log_per_s': r['evals']*tr/(raw['f64_ms']*1e-3) if raw['f64_ms'] else None,
+                                          'dd_ms': raw['dd_ms']}
+            ref = gold.get((name, h))
+            base = ref if ref is not None else (row['alldd']['value'] if 'alldd' in row else None)
+            row['reference_value'] = ref
+            row['error_vs'] = 'reference hsum (host dd oracle)' if ref is not None else ('all-dd GPU run' if base else None)
+            for form in ('fp64dd', 'fp64', 'alldd'):
+                if form in row and base:
+                    row[form]['rel_err'] = abs(row[form]['value'] - base)/abs(base)
+            rows.append(row)
+            print(json.dumps(row), flush=True)
+    clk = clocks.stop()
+    line = {'workload': 'synth', 'metric': 'synthetic Sinc-sum points/s, FP64+dd', 'unit': 'points/s',
+            'peak_fp64_tflops': peak, 'clocks': clk, 'cases': len(rows),
+            'config': {'workload': 'syn_d{5,8,11} at h in %s, N=2ceil(30/h)+1, eps=%g' % (list(SYN_H), EPS)}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -155,8 +275,20 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-alldd', action='store_true', help='skip the all-double-double comparison')
+    ap.add_argument('--workload', default='all3', choices=['all3', 'mixed', 'synth'],
+                    help='all3: the headline line; mixed: the mixed batch, one-at-a-time vs concurrent; '
+                         'synth: the synthetic microbenchmark and its precision table (one GPU)')
     args = ap.parse_args()
     rank, world, local = env_rank()
+    if args.workload != 'all3':
+        if rank == 0 and args.impl == 'ours':
+            from sincfeyn_b200 import sq
+            import ctypes as C
+            L = sq.lib()
+            L.sqb_timer_stop.restype = C.c_double
+            sq.kernel_timing(True)
+            (run_mixed if args.workload == 'mixed' else run_synth)(args, sq, L)
+        return
     if world > 1:
         import torch.distributed as dist
         import datetime

@@ -63,7 +63,14 @@ typedef struct {
     int device;            /* CUDA device (0) */
     long max_children;     /* children per device batch, 0 = default (2^25) */
     int verbose;           /* 1: timing lines on stderr */
+    double ckpt_every;     /* SINCQED_CKPT: > 0 writes a checkpoint at the end of every refinement level but the
+                              last and resumes from a matching one (driver/checkpoint.c:1-6); 0 = off (the
+                              library's default; the CLI's is the reference's 600) */
+    const char *ckpt_dir;  /* SINCQED_CKPT_DIR (NULL: the current directory) */
+    int ckpt_stop;         /* test hook: 1 = return SQB_CKPT_STOPPED right after the first checkpoint is written,
+                              as a run killed there would stop */
 } sqb_opts_t;
+#define SQB_CKPT_STOPPED 2 /* sqb_hsum's return code under ckpt_stop */
 
 /* res_t of the reference (driver/sq.h:111) and the per-graph log counters (driver/main.c:58-65) */
 typedef struct {
@@ -90,6 +97,25 @@ void sqb_default_opts(sqb_opts_t *o);
  * (driver/main.c:211-215).  Returns 0, or a nonzero error code (sqb_error() has the message). */
 int  sqb_hsum(const char *graph, double h, int N, double eps, int top, const sqb_opts_t *o, sqb_result_t *r);
 const char *sqb_error(void);
+
+/* Many integrals at once (no counterpart in the reference, whose driver runs one graph after another,
+ * driver/main.c:220-247): each job is one sqb_hsum(); `workers` host threads, each with its own CUDA
+ * stream and device buffers, take the jobs in descending `cost` (ties in list order) so that one
+ * integral's latency-bound top-level grow overlaps another's FP64 level passes.  Results and return
+ * codes per job (res[j], rcs[j]); *device_ms = device time of the whole batch (CUDA events: every worker
+ * stream waits on a start event of the caller's stream, which waits on every worker's end event).
+ * Returns 0, or the number of failed jobs (sqb_error() names the first). */
+typedef struct {
+    const char *graph;
+    double h; int N; double eps; int top;   /* as sqb_hsum; top < 0: the reference's default */
+    double cost;                            /* scheduling estimate (e.g. expected evaluations); 0: list order */
+} sqb_job_t;
+int  sqb_hsum_batch(const sqb_job_t *jobs, int n, const sqb_opts_t *o, int workers, sqb_result_t *res, int *rcs,
+                    double *device_ms);
+/* the batch tuner: runs the calibration jobs once per candidate worker count, rate[c] = evaluated points
+ * per second of device time; *best = the fastest candidate.  Returns 0 or a batch error. */
+int  sqb_batch_tune(const sqb_job_t *jobs, int n, const sqb_opts_t *o, const int *cand, int ncand, double *rate,
+                    int *best);
 
 /* the graphs compiled into this library: name, Volkov string, L, D, mirror weight */
 int  sqb_graph_count(void);
@@ -155,6 +181,35 @@ int  sqb_level_noalloc(const char *graph, double h, int K, const void *cells, lo
                        double pw, double thr, double abserr, double nearf, double ddslack,
                        int abskip, int abcheck, int dropunres, void *next, long next_cap,
                        double *sums, long long *counts, void *stream);
+
+/* ------------------------------------------------------------------------------------------------
+ * 4. Checkpoints in the reference's format SQCK4 (driver/checkpoint.c:59-120, ckpt_t at driver/sq.h:84-93):
+ *    the file sincqed_<graph>.ckpt that the reference writes and resumes from, field for field, so that
+ *    either program resumes the other's run.  sqb_hsum writes one at the end of every level but the last
+ *    (opts ckpt_every > 0): the next level's cells, streamed from the device in cell order, and the run's
+ *    sums; it resumes from a file whose header matches (name, h, eps, N, top, dim, K) and removes it when
+ *    the graph finishes.  The predictor table is written empty (vcap = 0: the predictor is off). */
+typedef struct {
+    char name[32]; double h, eps; int N, top, dim, k;    /* header ckhead_t (magic "SQCK4") */
+    int lev; long next;                                  /* level to refine next, first unprocessed cell */
+    double s, a, drop, u; long ne, q;                    /* sums of the level in progress (or just finished) */
+    double Slev[16]; int nl;
+    double S[3], Ah, ref, prune, trunc, unres, t;        /* res_t */
+    long nev, nq, kept_top;
+    long ncur; signed char *cur;                         /* cells, 12 bytes each (pt_t) */
+    long nnxt; signed char *nxt;
+    double es[5]; long cnt[3]; int esok;                 /* shadow sums and predictor check; counters */
+    int vsz; long vcap, vn; void *vs;                    /* the predictor's table: vcap slots of vsz bytes */
+} sqb_ckpt_t;
+#define SQB_CKPT_VSLOT 16  /* sizeof(vslot_t) of the reference (driver/sum.c:85) */
+/* write c to path atomically (path.tmp, then rename); 0 or -1 */
+int  sqb_ckpt_save(const char *path, const sqb_ckpt_t *c);
+/* read path into c (cur, nxt, vs allocated; free them with sqb_ckpt_free): 1 read, 0 absent, -1 damaged or
+ * another format */
+int  sqb_ckpt_load(const char *path, sqb_ckpt_t *c);
+void sqb_ckpt_free(sqb_ckpt_t *c);
+/* the file name the reference uses: <dir or .>/sincqed_<graph>.ckpt (driver/checkpoint.c:67-69) */
+void sqb_ckpt_name(char *buf, size_t n, const char *dir, const char *graph);
 
 #ifdef __cplusplus
 }

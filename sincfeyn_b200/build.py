@@ -144,14 +144,14 @@ def count_flops(graphs):
     src = os.path.join(GEN, 'count.cc')
     exe = os.path.join(BUILD, 'count')
     L = ['/* generated by sincfeyn_b200/build.py: algorithmic flop counter */',
-         '#include <stdio.h>', '#include "sqcount.h"', 'long sq_flops;',
+         '#include <stdio.h>', '#include "sqcount.h"', 'long sq_flops, sq_trans;',
          '#define SQ_TABLE static const', '#define SQ_FUNC', '#define SQ_CHUNK', '#define SQ_CHUNK_DD', '#define RABS(x) sq_rabs(x)',
          '#define SQ_EXP(x) sq_exp(x)', '#define SQ_LOG(x) sq_log(x)',
          '#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX) \\',
          'static void count_##NAME(void){ sq_count sf[D], ab; for(int d = 0; d < D; d++) sf[d] = sq_count(0.7 + 0.37*d); \\',
-         '  sq_flops = 0; sqg_##NAME::K<sq_count, 1>::f_##NAME(sf, &ab); long a1 = sq_flops; \\',
+         '  sq_flops = 0; sq_trans = 0; sqg_##NAME::K<sq_count, 1>::f_##NAME(sf, &ab); long a1 = sq_flops, t1 = sq_trans; \\',
          '  sq_flops = 0; sqg_##NAME::K<sq_count, 0>::f_##NAME(sf, &ab); long a0 = sq_flops; \\',
-         '  printf("%s\\"%s\\": {\\"ab1\\": %ld, \\"ab0\\": %ld}", first ? "" : ",\\n", #NAME, a1, a0); first = 0; }',
+         '  printf("%s\\"%s\\": {\\"ab1\\": %ld, \\"ab0\\": %ld, \\"tr\\": %ld}", first ? "" : ",\\n", #NAME, a1, a0, t1); first = 0; }',
          'static int first = 1;']
     for name, D, cuh, _ in graphs:
         L.append('#include "%s"' % os.path.basename(cuh))
@@ -188,10 +188,11 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     reg = write_registry(graphs, flops)
     hdrs = [os.path.join(CSRC, f) for f in ('sqkern.cuh', 'sqdd.cuh', 'sqb_internal.h', 'sqb_rt.h')] + \
            [os.path.join(INC, 'sincfeyn_b200.h')]
+    khdrs = [os.path.join(CSRC, f) for f in ('sqkern.cuh', 'sqdd.cuh', 'sqb_internal.h')]   # what a graph TU includes
     jobs_list = []
     for name, D, cuh, tu in graphs:
         o = os.path.join(OBJ, 'k_%s.o' % name)
-        if _newer(o, [tu, cuh] + hdrs):
+        if _newer(o, [tu, cuh] + khdrs):
             jobs_list.append([NVCC] + NVFLAGS + ['-I' + GEN, '-c', tu, '-o', o])
     rt_o = os.path.join(OBJ, 'runtime.o')
     if _newer(rt_o, [os.path.join(CSRC, 'runtime.cu')] + hdrs):
@@ -208,15 +209,21 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     eng_o = os.path.join(OBJ, 'engine.o')
     if _newer(eng_o, [os.path.join(CSRC, 'engine.cpp')] + hdrs):
         jobs_list.append([CXX] + CXXFLAGS + ['-c', os.path.join(CSRC, 'engine.cpp'), '-o', eng_o])
+    ck_o = os.path.join(OBJ, 'ckpt.o')
+    if _newer(ck_o, [os.path.join(CSRC, 'ckpt.cpp')] + hdrs):
+        jobs_list.append([CXX] + CXXFLAGS + ['-c', os.path.join(CSRC, 'ckpt.cpp'), '-o', ck_o])
+    bat_o = os.path.join(OBJ, 'batch.o')
+    if _newer(bat_o, [os.path.join(CSRC, 'batch.cpp')] + hdrs):
+        jobs_list.append([CXX] + CXXFLAGS + ['-pthread', '-c', os.path.join(CSRC, 'batch.cpp'), '-o', bat_o])
     n = jobs or min(len(jobs_list) or 1, os.cpu_count() or 4)
     if verbose and jobs_list:
         print('sincfeyn_b200: compiling %d objects with %d jobs' % (len(jobs_list), n), file=sys.stderr)
     with cf.ThreadPoolExecutor(max_workers=n) as ex:
         for f in [ex.submit(_run, c) for c in jobs_list]:
             f.result()
-    objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o]
+    objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o, bat_o, ck_o]
     if _newer(LIBSO, objs):
-        _run([NVCC] + ARCH + ['-shared', '-o', LIBSO] + objs + ['-Xcompiler', '-fopenmp', '-lgomp'])
+        _run([NVCC] + ARCH + ['-shared', '-o', LIBSO] + objs + ['-Xcompiler', '-fopenmp', '-lgomp', '-lpthread'])
     main_cpp = os.path.join(CSRC, 'main.cpp')
     if _newer(CLI, [main_cpp, LIBSO, os.path.join(INC, 'sincfeyn_b200.h')]):
         _run([CXX, '-O2', '-std=c++17', '-I' + INC, '-o', CLI, main_cpp, '-L' + LIB, '-lsqb200',

@@ -1,0 +1,172 @@
+/* batch.cpp -- many integrals at once: sqb_hsum_batch() and its tuner.
+ *
+ * A batch is a list of integrals (graph, h, N, eps, top), e.g. every graph of a class at several h.
+ * Each integral is one sqb_hsum() (the reference's hsum(), driver/sum.c:556-814), unchanged; the batch
+ * runs them concurrently from a pool of host worker threads.  Every worker owns a CUDA stream, its
+ * buffers and its share of device memory (the runtime's state is per thread), and pulls the next
+ * integral from a shared queue, largest estimated cost first (longest-processing-time order), so that
+ * the latency-bound parts of one integral (the top-level grow, which waits for every frontier's sums
+ * on the host) overlap the FP64-bound level passes of others and small integrals fill the gaps
+ * that a single integral's launches leave on the device.
+ *
+ * Device time: the caller's stream records a start event that every worker stream waits on before its
+ * first launch; every worker records an end event after its last; the caller's stream waits on all of
+ * them and records the stop event.  The elapsed time between start and stop is the batch's device time.
+ *
+ * The tuner runs a calibration list (normally a few integrals of the batch) once per candidate worker
+ * count and returns the count with the highest evaluated points per second of device time. */
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+#include <algorithm>
+#include <stdio.h>
+#include <string.h>
+#include <cuda_runtime.h>
+#include "sincfeyn_b200.h"
+#include "sqb_rt.h"
+
+extern "C" void sqb_set_error_msg(const char *msg);
+extern "C" void sqb_set_mem_share(double f);
+
+namespace {
+
+struct Batch {
+    const sqb_job_t *jobs = nullptr; int n = 0, nw = 0;
+    sqb_opts_t o;
+    sqb_result_t *res = nullptr; int *rcs = nullptr;
+    std::vector<int> order;
+    std::atomic<int> next{0};
+    cudaEvent_t start = nullptr;
+    std::vector<cudaEvent_t> ends;
+    std::vector<int> ended;          /* worker recorded its end event */
+    std::mutex m; std::condition_variable cv; int left = 0, failures = 0; std::string err;
+};
+
+/* the pool: workers wait for a new generation.  Its mutex and condition variable are never destroyed:
+ * the workers are detached and still wait on them when the process exits, and destroying a condition
+ * variable that has waiters blocks (glibc), which would hang the exit. */
+std::mutex &PM = *new std::mutex;
+std::condition_variable &PCV = *new std::condition_variable;
+Batch *CUR = nullptr;
+unsigned long GEN = 0;
+int NSTARTED = 0;
+const int MAXW = 32;
+
+void serve(Batch *b, int id){
+    sqb_set_mem_share(1.0/b->nw);
+    std::string err;
+    int ok = sqb_dev_init(b->o.device) == 0;
+    cudaStream_t s = ok ? (cudaStream_t)sqb_dev_stream() : nullptr;
+    if(ok && cudaStreamWaitEvent(s, b->start, 0) != cudaSuccess) ok = 0;
+    if(!ok) err = std::string("worker ") + std::to_string(id) + ": " + sqb_last_error();
+    while(ok){
+        const int k = b->next.fetch_add(1);
+        if(k >= b->n) break;
+        const int j = b->order[k];
+        const sqb_job_t &J = b->jobs[j];
+        b->rcs[j] = sqb_hsum(J.graph, J.h, J.N, J.eps, J.top, &b->o, &b->res[j]);
+        if(b->rcs[j]){
+            std::lock_guard<std::mutex> lk(b->m);
+            b->failures++;
+            if(b->err.empty()) b->err = std::string(J.graph) + ": " + sqb_error();
+        }
+    }
+    int rec = ok && cudaEventRecord(b->ends[id], s) == cudaSuccess;
+    std::lock_guard<std::mutex> lk(b->m);
+    b->ended[id] = rec;
+    if(!err.empty()){ b->failures++; if(b->err.empty()) b->err = err; }
+    if(--b->left == 0) b->cv.notify_all();
+}
+
+void worker(int id){
+    unsigned long seen = 0;
+    for(;;){
+        Batch *b; int nw;
+        {
+            std::unique_lock<std::mutex> lk(PM);
+            PCV.wait(lk, [&]{ return GEN != seen; });
+            seen = GEN; b = CUR; nw = b ? b->nw : 0;     /* read under the lock: b outlives only its workers */
+        }
+        if(id < nw) serve(b, id);
+    }
+}
+
+}  // namespace
+
+extern "C" int sqb_hsum_batch(const sqb_job_t *jobs, int n, const sqb_opts_t *o_in, int workers,
+                              sqb_result_t *res, int *rcs, double *device_ms){
+    static std::mutex one;            /* one batch at a time */
+    std::lock_guard<std::mutex> guard(one);
+    if(device_ms) *device_ms = 0;
+    if(n <= 0) return 0;
+    sqb_opts_t o; if(o_in) o = *o_in; else sqb_default_opts(&o);
+    if(workers < 1) workers = 1;
+    if(workers > MAXW) workers = MAXW;
+    if(workers > n) workers = n;
+    if(sqb_dev_init(o.device)){ sqb_set_error_msg(sqb_last_error()); return -1; }
+    for(int j = 0; j < n; j++){
+        if(!sqb_find_graph(jobs[j].graph)){
+            char m[256]; snprintf(m, sizeof m, "unknown graph %s", jobs[j].graph); sqb_set_error_msg(m); return -1;
+        }
+        rcs[j] = 0; memset(&res[j], 0, sizeof res[j]);
+    }
+    Batch b;
+    b.jobs = jobs; b.n = n; b.nw = workers; b.o = o; b.res = res; b.rcs = rcs; b.left = workers;
+    b.order.resize(n);
+    for(int j = 0; j < n; j++) b.order[j] = j;
+    std::stable_sort(b.order.begin(), b.order.end(), [&](int x, int y){ return jobs[x].cost > jobs[y].cost; });
+    b.ends.assign(workers, nullptr); b.ended.assign(workers, 0);
+    cudaStream_t s = (cudaStream_t)sqb_dev_stream();
+    int rc = 0;
+    if(cudaEventCreate(&b.start) != cudaSuccess) rc = -1;
+    for(int i = 0; i < workers && !rc; i++) if(cudaEventCreate(&b.ends[i]) != cudaSuccess) rc = -1;
+    if(!rc && cudaEventRecord(b.start, s) != cudaSuccess) rc = -1;
+    if(rc){
+        sqb_set_error_msg("sqb_hsum_batch: event setup failed");
+        if(b.start) cudaEventDestroy(b.start);
+        for(cudaEvent_t e : b.ends) if(e) cudaEventDestroy(e);
+        return -1;
+    }
+    {
+        std::lock_guard<std::mutex> lk(PM);
+        while(NSTARTED < workers){ std::thread(worker, NSTARTED).detach(); NSTARTED++; }
+        CUR = &b; GEN++;
+    }
+    PCV.notify_all();
+    {
+        std::unique_lock<std::mutex> lk(b.m);
+        b.cv.wait(lk, [&]{ return b.left == 0; });
+    }
+    { std::lock_guard<std::mutex> lk(PM); CUR = nullptr; }
+    for(int i = 0; i < workers; i++) if(b.ended[i]) cudaStreamWaitEvent(s, b.ends[i], 0);
+    cudaEvent_t stop = nullptr;
+    if(cudaEventCreate(&stop) == cudaSuccess && cudaEventRecord(stop, s) == cudaSuccess && cudaEventSynchronize(stop) == cudaSuccess){
+        float t = 0; cudaEventElapsedTime(&t, b.start, stop);
+        if(device_ms) *device_ms = t;
+    }
+    if(stop) cudaEventDestroy(stop);
+    cudaEventDestroy(b.start);
+    for(cudaEvent_t e : b.ends) cudaEventDestroy(e);
+    if(b.failures){ sqb_set_error_msg(b.err.c_str()); return b.failures; }
+    return 0;
+}
+
+extern "C" int sqb_batch_tune(const sqb_job_t *jobs, int n, const sqb_opts_t *o, const int *cand, int ncand,
+                              double *rate, int *best){
+    *best = 0;
+    std::vector<sqb_result_t> res(n > 0 ? n : 1);
+    std::vector<int> rcs(n > 0 ? n : 1);
+    double top = -1;
+    for(int c = 0; c < ncand; c++){
+        double ms = 0;
+        int rc = sqb_hsum_batch(jobs, n, o, cand[c], res.data(), rcs.data(), &ms);
+        if(rc) return rc;
+        double ev = 0; for(int j = 0; j < n; j++) ev += (double)res[j].nev;
+        rate[c] = ms > 0 ? ev/(ms*1e-3) : 0;
+        if(rate[c] > top){ top = rate[c]; *best = cand[c]; }
+    }
+    return 0;
+}

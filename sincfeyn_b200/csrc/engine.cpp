@@ -34,7 +34,9 @@
 #include "sqb_rt.h"
 #include "sincfeyn_b200.h"
 
-static char E_[512];
+static thread_local char E_[512];
+static thread_local double MEMSHARE = 1.0;    /* share of device memory for this thread's cell lists */
+extern "C" void sqb_set_mem_share(double f){ MEMSHARE = f > 0 && f <= 1 ? f : 1.0; }
 extern "C" const char *sqb_error(void){ return E_; }
 extern "C" void sqb_set_error_msg(const char *msg){ snprintf(E_, sizeof E_, "%s", msg); }
 #define FAIL(...) do { snprintf(E_, sizeof E_, __VA_ARGS__); return -1; } while(0)
@@ -184,44 +186,83 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
         else { R.X[k + K] = exp(k*h); R.Wt[k + K] = R.X[k + K]*h; }
     }
     if(sqb_dev_tables(R.X.data(), R.Wt.data(), K)) FAIL("device: %s", sqb_last_error());
-    const double t0 = now();
+    double t0 = now();
     const unsigned long long l0 = sqb_launch_count() + sqb_top_launches();
     { double a, b; long c; sqb_kernel_times(&a, &b, &c, 1); }
-    set_test(R, R.o.abserr0);
-    int zero = 0;
-    if(box_zero(R, top, &res->nev, &zero)) return -1;
-    if(zero){ res->zero = 1; res->t = now() - t0; return 0; }
-    GrowOut go; sqb_pt_t *dcur = NULL; long ncur = 0;
-    if(grow(R, top, eps*1e-3, &go, &dcur, &ncur)) return -1;
-    res->nev += go.nev; res->ref = go.A; res->prune = go.drop;
-    if(top == 0 && go.gshn) res->prune = fabs(go.gshs);
-    if(go.A == 0){ sqb_dev_free(dcur); res->t = now() - t0; res->nq = R.nq; res->unresdrop = R.unresdrop; return 0; }
-    { double r = go.e2 > 0 ? go.e1/go.e2 : 0; res->trunc = (r > 0 && r < 1) ? go.e1*r/(1 - r) : go.e1; }
+    /* a checkpoint of this run (same graph, h, eps, N, top, D, K) resumes it (driver/sum.c:596-606) */
+    char ckfn[4096] = ""; sqb_ckpt_t ck; memset(&ck, 0, sizeof ck); int resumed = 0;
+    if(R.o.ckpt_every > 0){
+        sqb_ckpt_name(ckfn, sizeof ckfn, R.o.ckpt_dir, R.g->name);
+        const int lr = sqb_ckpt_load(ckfn, &ck);
+        if(lr == 1 && !strcmp(ck.name, R.g->name) && ck.h == h && ck.eps == eps && ck.N == N && ck.top == top &&
+           ck.dim == R.D && ck.k == K && ck.lev >= 0 && ck.lev < top && ck.next >= 0 && ck.next <= ck.ncur && ck.nl >= 1) resumed = 1;
+        else {
+            if(lr == 1) sqb_ckpt_free(&ck);
+            if(lr && R.o.verbose) fprintf(stderr, "# checkpoint %s is for a different run or damaged: ignored\n", ckfn);
+        }
+    }
+    sqb_pt_t *dcur = NULL; long ncur = 0;
+    double Slev[16]; int nl = 0; int esok, lev0 = top - 1; long cnext = 0;
+    sqb_acc_t acc0; memset(&acc0, 0, sizeof acc0);
     for(int i = 0; i < 3; i++) res->S[i] = NAN;
-    double Slev[16]; int nl = 0; Slev[nl++] = go.S;
-    res->kept_top = ncur;
-    res->t_top = now() - t0;
-    const int esok = R.D < SQB_MAXD && top > 0;
+    if(resumed){
+        res->nev = ck.nev; res->ref = ck.ref; res->prune = ck.prune; res->trunc = ck.trunc; res->kept_top = ck.kept_top;
+        R.nq = ck.nq; res->abskipped = ck.cnt[1];
+        nl = ck.nl; for(int i = 0; i < nl; i++) Slev[i] = ck.Slev[i];
+        esok = ck.esok; lev0 = ck.lev; cnext = ck.next; t0 -= ck.t;
+        ncur = ck.ncur;
+        dcur = (sqb_pt_t*)sqb_dev_alloc((size_t)(ncur ? ncur : 1)*sizeof(sqb_pt_t));
+        if(!dcur || (ncur && sqb_dev_upload(dcur, ck.cur, (size_t)ncur*sizeof(sqb_pt_t)))){
+            sqb_dev_free(dcur); sqb_ckpt_free(&ck); FAIL("device copy of the checkpoint's %ld cells failed", ncur); }
+        if(cnext > 0){         /* a level in progress: its partial sums carry on */
+            acc0.S[0] = ck.s; acc0.A[0] = ck.a; acc0.drop[0] = ck.drop; acc0.u[0] = ck.u;
+            acc0.b1[0] = ck.es[0]; acc0.b2[0] = ck.es[1]; acc0.ne = ck.ne; acc0.nq = ck.q;
+        }
+        if(R.o.verbose) fprintf(stderr, "# resuming %s from checkpoint: refine to step %dh, cell %ld of %ld\n",
+                                R.g->name, 1 << ck.lev, ck.next, ck.ncur);
+        res->t_top = 0;
+    } else {
+        set_test(R, R.o.abserr0);
+        int zero = 0;
+        if(box_zero(R, top, &res->nev, &zero)) return -1;
+        if(zero){ res->zero = 1; res->t = now() - t0; return 0; }
+        GrowOut go;
+        if(grow(R, top, eps*1e-3, &go, &dcur, &ncur)) return -1;
+        res->nev += go.nev; res->ref = go.A; res->prune = go.drop;
+        if(top == 0 && go.gshn) res->prune = fabs(go.gshs);
+        if(go.A == 0){ sqb_dev_free(dcur); res->t = now() - t0; res->nq = R.nq; res->unresdrop = R.unresdrop; return 0; }
+        { double r = go.e2 > 0 ? go.e1/go.e2 : 0; res->trunc = (r > 0 && r < 1) ? go.e1*r/(1 - r) : go.e1; }
+        Slev[nl++] = go.S;
+        res->kept_top = ncur;
+        res->t_top = now() - t0;
+        esok = R.D < SQB_MAXD && top > 0;
+    }
     /* the levels on the device */
     set_test(R, fmax(R.o.abserr0, R.o.abrel*eps*res->ref));    /* driver/sum.c:651 */
     sqb_pt_t *dnext = NULL; long next_cap = 0;
     const double tl0 = now(); double es1 = 0, es2 = 0, ah = 0, uu = 0;
-    for(int lev = top - 1; lev >= 0; lev--){
+    for(int lev = lev0; lev >= 0; lev--){
         const int st = 1 << lev, last = lev == 0;
+        /* resumed in mid-level: cells [cnext, ncur) remain, and the checkpoint's kept cells come first */
+        const long nkeep0 = lev == lev0 ? ck.nnxt : 0, c0 = lev == lev0 ? cnext : 0;
         sqb_level_t L; memset(&L, 0, sizeof L);
-        L.g = R.g; L.cells = dcur; L.ncell = ncur; L.st = st; L.last = last;
+        L.g = R.g; L.cells = dcur + c0; L.ncell = ncur - c0; L.st = st; L.last = last;
         L.pw = pow(st, R.D); L.thr = eps*res->ref*1e-2; L.t = R.t; L.max_children = R.o.max_children;
         if(!last){
-            double want = (double)ncur*(double)(1L << R.D);
-            double room = 0.35*(double)sqb_dev_total_bytes()/sizeof(sqb_pt_t);
+            double want = (double)(ncur - c0)*(double)(1L << R.D) + nkeep0;
+            double room = 0.35*MEMSHARE*(double)sqb_dev_total_bytes()/sizeof(sqb_pt_t);
             next_cap = (long)(want < room ? want : room) + 1;
             dnext = (sqb_pt_t*)sqb_dev_alloc(next_cap*sizeof(sqb_pt_t));
-            if(!dnext){ sqb_dev_free(dcur); FAIL("device allocation of the next level (%ld cells) failed", next_cap); }
-            L.next = dnext; L.next_cap = next_cap;
+            if(!dnext){ sqb_dev_free(dcur); sqb_ckpt_free(&ck); FAIL("device allocation of the next level (%ld cells) failed", next_cap); }
+            if(nkeep0 && (nkeep0 >= next_cap || sqb_dev_upload(dnext, ck.nxt, (size_t)nkeep0*sizeof(sqb_pt_t)))){
+                sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); FAIL("device copy of the checkpoint's kept cells failed"); }
+            L.next = dnext + nkeep0; L.next_cap = next_cap - nkeep0;
         }
-        sqb_acc_t acc; memset(&acc, 0, sizeof acc); long nn = 0; double ms = 0;
-        if(sqb_dev_level(&L, &acc, &nn, &ms)){ sqb_dev_free(dcur); sqb_dev_free(dnext); FAIL("device: %s", sqb_last_error()); }
-        if(acc.overflow){ sqb_dev_free(dcur); sqb_dev_free(dnext); FAIL("level %d: %ld kept cells exceed the device list (%ld)", lev, nn, next_cap); }
+        sqb_acc_t acc; if(lev == lev0) acc = acc0; else memset(&acc, 0, sizeof acc);
+        long nn = 0; double ms = 0;
+        if(sqb_dev_level(&L, &acc, &nn, &ms)){ sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); FAIL("device: %s", sqb_last_error()); }
+        if(acc.overflow){ sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); FAIL("level %d: %ld kept cells exceed the device list (%ld)", lev, nn, next_cap); }
+        nn += nkeep0;
         Slev[nl++] = ddv(acc.S);
         res->prune += ddv(acc.drop); res->nev += (long)acc.ne; R.nq += (long)acc.nq; R.unresdrop += (long)acc.unres;
         res->abskipped += (long)acc.skipped;
@@ -229,9 +270,36 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
         if(last){ ah = ddv(acc.A); uu = ddv(acc.u); es1 = ddv(acc.b1); es2 = ddv(acc.b2); }
         if(R.o.verbose) fprintf(stderr, "# %s level step %dh: %ld cells, %llu evals, %llu fallback, %ld kept, %.1f ms\n",
                                 R.g->name, st, ncur, acc.ne, acc.nq, nn, ms);
+        if(R.o.ckpt_every > 0 && !last){
+            /* the state between this level and the next, as the reference saves it (driver/sum.c:797-799) */
+            std::vector<sqb_pt_t> host((size_t)nn);
+            if(nn && sqb_dev_download(host.data(), dnext, (size_t)nn*sizeof(sqb_pt_t))){
+                sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); FAIL("device: %s", sqb_last_error()); }
+            sqb_ckpt_t c; memset(&c, 0, sizeof c);
+            snprintf(c.name, sizeof c.name, "%s", R.g->name);
+            c.h = h; c.eps = eps; c.N = N; c.top = top; c.dim = R.D; c.k = K;
+            c.lev = lev - 1; c.next = 0;
+            c.s = Slev[nl - 1]; c.a = ddv(acc.A); c.drop = ddv(acc.drop); c.u = ddv(acc.u);
+            c.ne = (long)acc.ne; c.q = (long)acc.nq;
+            for(int i = 0; i < nl; i++) c.Slev[i] = Slev[i];
+            c.nl = nl;
+            c.ref = res->ref; c.prune = res->prune; c.trunc = res->trunc; c.t = now() - t0;
+            c.nev = res->nev; c.nq = R.nq; c.kept_top = res->kept_top;
+            c.ncur = nn; c.cur = (signed char*)host.data();
+            c.cnt[1] = res->abskipped; c.esok = esok;
+            c.vsz = SQB_CKPT_VSLOT;
+            if(sqb_ckpt_save(ckfn, &c) && R.o.verbose) fprintf(stderr, "# warning: could not write checkpoint %s\n", ckfn);
+            if(R.o.ckpt_stop){
+                sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck);
+                snprintf(E_, sizeof E_, "stopped after the checkpoint %s (ckpt_stop)", ckfn);
+                return SQB_CKPT_STOPPED;
+            }
+        }
         sqb_dev_free(dcur); dcur = dnext; dnext = NULL; ncur = last ? 0 : nn;
     }
     sqb_dev_free(dcur);
+    sqb_ckpt_free(&ck);
+    if(R.o.ckpt_every > 0) remove(ckfn);          /* the graph is finished (driver/sum.c:804) */
     res->t_levels = now() - tl0;
     if(top > 0){ res->unres = sqrt(uu); res->Ah = ah; }
     else res->unres = R.u;            /* top = 0: the grow's sum of squares as it stands (driver/sum.c:795) */

@@ -67,6 +67,10 @@ int main(int argc, char **argv){
     if((e = getenv("SQB_ALLDD"))) o.alldd = atoi(e);
     if((e = getenv("SQB_DEVICE"))) o.device = atoi(e);
     if((e = getenv("SQB_VERBOSE"))) o.verbose = atoi(e);
+    /* checkpoints at every level end, on by default as in the reference (driver/main.c:28,184) */
+    o.ckpt_every = 600;
+    if((e = getenv("SINCQED_CKPT"))) o.ckpt_every = atof(e);
+    o.ckpt_dir = getenv("SINCQED_CKPT_DIR");
     const int NG = sqb_graph_count();
     if(argc < 2 || !strcmp(argv[1], "list")){
         printf("%d graphs (one per mirror pair; w = mirror weight), precision fallback double-double on the GPU\n", NG);

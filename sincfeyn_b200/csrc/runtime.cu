@@ -22,12 +22,17 @@
 #include <omp.h>
 #include "sqb_rt.h"
 #include "sqdd.cuh"
+#include <atomic>
 #include "sincfeyn_b200.h"
 
 extern "C" const sqb_graph_t *const SQB_ALL[];
 extern "C" const int SQB_NALL;
 
-static char g_err[512];
+/* Every piece of state below is per host thread (thread_local): each thread that calls the chosen form
+ * has its own stream, events, buffers and error text, so several integrals can run concurrently from
+ * a pool of threads (batch.cpp).  The plain form (gpu_setup ... gpu_wait) stays single-threaded, as the
+ * reference's driver calls it (driver/eval.c:104-107). */
+static thread_local char g_err[512];
 #define CKR(x) do { cudaError_t e_ = (x); if(e_ != cudaSuccess){                                    \
     snprintf(g_err, sizeof g_err, "%s at %s:%d: %s", #x, __FILE__, __LINE__, cudaGetErrorString(e_)); \
     return (int)e_; } } while(0)
@@ -63,10 +68,8 @@ typedef struct {
 
 struct Dev {
     int on, dev, nsm;
-    unsigned long long h2d, d2h;  /* bytes copied by the chosen form's calls */
     cudaEvent_t t0, t1; void *flush; size_t flushn;
     unsigned long long launches;   /* kernels of this library launched so far */
-    int ktime;                     /* time the FP64 and dd kernels of the level passes with events */
     cudaEvent_t k0, k1, d1;
     double f64_ms, dd_ms; long f64_n;
     char info[256];
@@ -80,7 +83,9 @@ struct Dev {
     long dcap; sqb_pt_t *dpts; unsigned char *dskip;
     long hcap; sqb_pt_t *hpts; unsigned char *hskip, *hst; double *hv, *huu;
 };
-static Dev G;
+static thread_local Dev G;
+static int KTIME;                  /* sqb_kernel_timing(): all threads */
+static std::atomic<unsigned long long> H2D, D2H;   /* bytes copied by the chosen form's calls, all threads */
 
 extern "C" int sqb_dev_init(int device){
     if(G.on) return 0;
@@ -116,7 +121,7 @@ extern "C" int sqb_dev_tables(const double *X, const double *Wt, int K){
     }
     CKR(cudaMemcpy(G.X, X, nt*sizeof(double), cudaMemcpyHostToDevice));
     CKR(cudaMemcpy(G.Wt, Wt, nt*sizeof(double), cudaMemcpyHostToDevice));
-    G.h2d += 2*nt*sizeof(double);
+    H2D += 2*nt*sizeof(double);
     G.K = K;
     return 0;
 }
@@ -162,16 +167,16 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
         return 0;
     }
     CKR(cudaMemsetAsync(G.nfb, 0, sizeof(unsigned long long), G.s));
-    if(G.ktime) CKR(cudaEventRecord(G.k0, G.s));
+    if(KTIME) CKR(cudaEventRecord(G.k0, G.s));
     g->f64(a, grid_for(g, 0, npts, smem), 128, smem, G.s);
     CKR(cudaGetLastError());
-    if(G.ktime) CKR(cudaEventRecord(G.k1, G.s));
+    if(KTIME) CKR(cudaEventRecord(G.k1, G.s));
     d.list = G.fb; d.nlist = G.nfb; d.listcap = G.cap; d.all = 0;
     /* the queue length is known only on the device: a persistent grid reads it */
     g->dd(&d, grid_for(g, 1, 1L << 30, smem), 128, smem, G.s);
     CKR(cudaGetLastError());
     G.launches += 2;
-    if(G.ktime){
+    if(KTIME){
         CKR(cudaEventRecord(G.d1, G.s));
         CKR(cudaEventSynchronize(G.d1));
         float x = 0, y = 0; cudaEventElapsedTime(&x, G.k0, G.k1); cudaEventElapsedTime(&y, G.k1, G.d1);
@@ -200,7 +205,7 @@ extern "C" int sqb_dev_eval_nodes(const sqb_graph_t *g, long n, const sqb_pt_t *
         memcpy(G.hpts, pts + i0, m*sizeof(sqb_pt_t));
         CKR(cudaMemcpyAsync(G.dpts, G.hpts, m*sizeof(sqb_pt_t), cudaMemcpyHostToDevice, G.s));
         if(skip){ memcpy(G.hskip, skip + i0, m); CKR(cudaMemcpyAsync(G.dskip, G.hskip, m, cudaMemcpyHostToDevice, G.s)); }
-        G.h2d += m*sizeof(sqb_pt_t) + (skip ? m : 0); G.d2h += m*(2*sizeof(double) + 1);
+        H2D += m*sizeof(sqb_pt_t) + (skip ? m : 0); D2H += m*(2*sizeof(double) + 1);
         sqb_eval_t a; memset(&a, 0, sizeof a); fill_eval(&a, t);
         a.pts = G.dpts; a.n = m; a.esize = 1; a.stride = SQB_MAXD; a.flag_at = -1; a.cells = 0; a.st = 0;
         a.skip = skip ? G.dskip : NULL;
@@ -243,7 +248,7 @@ extern "C" int sqb_dev_eval_resident(const sqb_graph_t *g, const sqb_pt_t *pts, 
     CKR(cudaMemcpyAsync(G.hst, G.stt, n, cudaMemcpyDeviceToHost, G.s));
     CKR(cudaMemcpyAsync(G.huu, G.uu, n*sizeof(double), cudaMemcpyDeviceToHost, G.s));
     CKR(cudaStreamSynchronize(G.s));
-    G.d2h += n*(2*sizeof(double) + 1);
+    D2H += n*(2*sizeof(double) + 1);
     long q = 0, nd = 0; double uu = 0;
     memcpy(v, G.hv, n*sizeof(double)); memcpy(stt, G.hst, n);
     for(long i = 0; i < n; i++){
@@ -275,7 +280,7 @@ extern "C" int sqb_preload(const char *graph){
 /* instrumentation: kernels launched so far; with ktime on, the FP64 and double-double kernels of every
  * evaluation pass are bracketed by events (one synchronisation per batch) and their times summed */
 extern "C" unsigned long long sqb_launch_count(void){ return G.launches; }
-extern "C" void sqb_kernel_timing(int on){ G.ktime = on; }
+extern "C" void sqb_kernel_timing(int on){ KTIME = on; }
 extern "C" void sqb_kernel_times(double *f64_ms, double *dd_ms, long *f64_launches, int reset){
     *f64_ms = G.f64_ms; *dd_ms = G.dd_ms; *f64_launches = G.f64_n;
     if(reset){ G.f64_ms = G.dd_ms = 0; G.f64_n = 0; }
@@ -473,7 +478,7 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
     sqb_acc_t h;
     CKR(cudaMemcpyAsync(&h, G.acc, sizeof h, cudaMemcpyDeviceToHost, G.s));
     CKR(cudaStreamSynchronize(G.s));
-    G.d2h += sizeof h;
+    D2H += sizeof h;
     float t = 0; cudaEventElapsedTime(&t, G.e0, G.e1); if(ms) *ms = t;
     double *src[6] = {h.S, h.A, h.drop, h.b1, h.b2, h.u}, *dst[6] = {acc->S, acc->A, acc->drop, acc->b1, acc->b2, acc->u};
     for(int q = 0; q < 6; q++){ sqdd x = sqdd(dst[q][0], dst[q][1]) + sqdd(src[q][0], src[q][1]); dst[q][0] = x.hi; dst[q][1] = x.lo; }
@@ -484,13 +489,15 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
 
 extern "C" void *sqb_dev_alloc(size_t bytes){ void *p = NULL; if(cudaMallocAsync(&p, bytes ? bytes : 16, G.s) != cudaSuccess){ cudaGetLastError(); return NULL; } return p; }
 extern "C" void sqb_dev_free(void *p){ if(p) cudaFreeAsync(p, G.s); }
-extern "C" int sqb_dev_upload(void *dst, const void *src, size_t bytes){ CKR(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice)); G.h2d += bytes; return 0; }
-extern "C" int sqb_dev_download(void *dst, const void *src, size_t bytes){ CKR(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost)); G.d2h += bytes; return 0; }
-extern "C" void sqb_dev_count_copy(unsigned long long h2d, unsigned long long d2h){ G.h2d += h2d; G.d2h += d2h; }
+extern "C" int sqb_dev_upload(void *dst, const void *src, size_t bytes){
+    CKR(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, G.s)); CKR(cudaStreamSynchronize(G.s)); H2D += bytes; return 0; }
+extern "C" int sqb_dev_download(void *dst, const void *src, size_t bytes){
+    CKR(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, G.s)); CKR(cudaStreamSynchronize(G.s)); D2H += bytes; return 0; }
+extern "C" void sqb_dev_count_copy(unsigned long long h2d, unsigned long long d2h){ H2D += h2d; D2H += d2h; }
 
 /* measurement helpers: bytes copied between host and device so far; events on the library's stream
  * around a region of work (device milliseconds); an L2 flush (a memset larger than L2) on that stream */
-extern "C" void sqb_copy_bytes(unsigned long long *h2d, unsigned long long *d2h){ *h2d = G.h2d; *d2h = G.d2h; }
+extern "C" void sqb_copy_bytes(unsigned long long *h2d, unsigned long long *d2h){ *h2d = H2D.load(); *d2h = D2H.load(); }
 extern "C" int sqb_timer_start(void){ if(sqb_dev_init(0)) return -1; CKR(cudaEventRecord(G.t0, G.s)); return 0; }
 extern "C" double sqb_timer_stop(void){
     if(cudaEventRecord(G.t1, G.s) != cudaSuccess || cudaEventSynchronize(G.t1) != cudaSuccess) return -1;

@@ -28,7 +28,7 @@
 #define SEEN 0xFFFFFFFFu
 #define CLAIM(id) (0xFFFFFFFEu - (unsigned)(id))
 
-static char terr[512];
+static thread_local char terr[512];   /* the state of this file is per host thread, like the runtime's */
 #define TCK(x) do { cudaError_t e_ = (x); if(e_ != cudaSuccess){                                    \
     snprintf(terr, sizeof terr, "%s at %s:%d: %s", #x, __FILE__, __LINE__, cudaGetErrorString(e_));   \
     return (int)e_; } } while(0)
@@ -112,13 +112,13 @@ __global__ void __launch_bounds__(TG_T) k_scatter(Op op, long n, const unsigned 
 }
 
 struct Scratch { unsigned *bcnt; unsigned long long *boff, *tot; long nbcap; };
-static Scratch SC;
-static cudaStream_t TS;
+static thread_local Scratch SC;
+static thread_local cudaStream_t TS;
 /* stream-ordered allocation from the device's memory pool: no device-wide synchronisation, and the pool
  * keeps freed memory for the next integral (the runtime sets its release threshold) */
 #define DMALLOC(p, n) cudaMallocAsync((void**)(p), (n), TS)
 #define DFREE(p) cudaFreeAsync((p), TS)
-static unsigned long long TL;    /* kernels launched by this file */
+static thread_local unsigned long long TL;    /* kernels launched by this file */
 extern "C" unsigned long long sqb_top_launches(void){ return TL; }
 extern "C" void sqb_dev_count_copy(unsigned long long h2d, unsigned long long d2h);
 
@@ -163,7 +163,7 @@ struct Grow {
     unsigned long long *err;
     int gs, abskip;
 };
-static Grow GR;
+static thread_local Grow GR;
 
 __global__ void k_rehash(const unsigned long long *ok, const unsigned *ow, long ocap, unsigned long long *key,
                          unsigned *word, unsigned long long mask, unsigned long long *err){

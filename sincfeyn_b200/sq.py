@@ -22,7 +22,8 @@ class Opts(C.Structure):
     """sqb_opts_t: the reference's environment settings that reach the hot path (driver/main.c:176-185)."""
     _fields_ = [('abserr0', C.c_double), ('abrel', C.c_double), ('nearf', C.c_double), ('ddslack', C.c_double),
                 ('abskip', C.c_int), ('abcheck', C.c_int), ('dropunres', C.c_int), ('growskip', C.c_int),
-                ('alldd', C.c_int), ('device', C.c_int), ('max_children', C.c_long), ('verbose', C.c_int)]
+                ('alldd', C.c_int), ('device', C.c_int), ('max_children', C.c_long), ('verbose', C.c_int),
+                ('ckpt_every', C.c_double), ('ckpt_dir', C.c_char_p), ('ckpt_stop', C.c_int)]
 
 
 class Result(C.Structure):
@@ -35,6 +36,12 @@ class Result(C.Structure):
                 ('t_top', C.c_double), ('t_levels', C.c_double), ('nlev', C.c_int),
                 ('lev_evals', C.c_long * 16), ('lev_ms', C.c_double * 16),
                 ('f64_ms', C.c_double), ('dd_ms', C.c_double), ('f64_launches', C.c_long), ('launches', C.c_long)]
+
+
+class Job(C.Structure):
+    """sqb_job_t: one integral of a batch."""
+    _fields_ = [('graph', C.c_char_p), ('h', C.c_double), ('N', C.c_int), ('eps', C.c_double), ('top', C.c_int),
+                ('cost', C.c_double)]
 
 
 class SqbError(RuntimeError):
@@ -67,6 +74,10 @@ def lib():
         L.sqb_probe_fp64.argtypes = [C.c_int, C.c_long]
         L.sqb_probe_fp64.restype = C.c_double
         L.gpu_info.restype = C.c_char_p
+        L.sqb_hsum_batch.argtypes = [C.POINTER(Job), C.c_int, C.POINTER(Opts), C.c_int, C.POINTER(Result),
+                                     C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.sqb_batch_tune.argtypes = [C.POINTER(Job), C.c_int, C.POINTER(Opts), C.POINTER(C.c_int), C.c_int,
+                                     C.POINTER(C.c_double), C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -75,8 +86,72 @@ def default_opts(**kw):
     o = Opts()
     lib().sqb_default_opts(C.byref(o))
     for k, v in kw.items():
-        setattr(o, k, v)
+        setattr(o, k, v.encode() if isinstance(v, str) else v)
     return o
+
+
+CKPT_STOPPED = 2
+
+
+class Checkpoint(C.Structure):
+    """sqb_ckpt_t: the reference's checkpoint (SQCK4), field for field."""
+    _fields_ = [('name', C.c_char * 32), ('h', C.c_double), ('eps', C.c_double), ('N', C.c_int), ('top', C.c_int),
+                ('dim', C.c_int), ('k', C.c_int), ('lev', C.c_int), ('next', C.c_long),
+                ('s', C.c_double), ('a', C.c_double), ('drop', C.c_double), ('u', C.c_double),
+                ('ne', C.c_long), ('q', C.c_long), ('Slev', C.c_double * 16), ('nl', C.c_int),
+                ('S', C.c_double * 3), ('Ah', C.c_double), ('ref', C.c_double), ('prune', C.c_double),
+                ('trunc', C.c_double), ('unres', C.c_double), ('t', C.c_double),
+                ('nev', C.c_long), ('nq', C.c_long), ('kept_top', C.c_long),
+                ('ncur', C.c_long), ('cur', C.POINTER(C.c_byte)), ('nnxt', C.c_long), ('nxt', C.POINTER(C.c_byte)),
+                ('es', C.c_double * 5), ('cnt', C.c_long * 3), ('esok', C.c_int),
+                ('vsz', C.c_int), ('vcap', C.c_long), ('vn', C.c_long), ('vs', C.c_void_p)]
+
+
+def ckpt_load(path):
+    """Read a checkpoint file: None if absent; a dict of its fields, the cell lists as (n, 12) int8 arrays."""
+    L = lib()
+    L.sqb_ckpt_load.argtypes = [C.c_char_p, C.POINTER(Checkpoint)]
+    L.sqb_ckpt_free.argtypes = [C.POINTER(Checkpoint)]
+    c = Checkpoint()
+    rc = L.sqb_ckpt_load(path.encode(), C.byref(c))
+    if rc == 0:
+        return None
+    if rc < 0:
+        raise SqbError('%s: damaged or not SQCK4' % path)
+    d = {f: getattr(c, f) for f, _ in Checkpoint._fields_ if f not in ('cur', 'nxt', 'vs')}
+    d['name'] = c.name.decode()
+    for f in ('Slev', 'S', 'es', 'cnt'):
+        d[f] = list(d[f])
+    for f, n in (('cur', c.ncur), ('nxt', c.nnxt)):
+        d[f] = np.ctypeslib.as_array(getattr(c, f), shape=(n * 12,)).reshape(n, 12).copy() if n else np.zeros((0, 12), np.int8)
+    L.sqb_ckpt_free(C.byref(c))
+    return d
+
+
+def ckpt_save(path, d):
+    """Write a checkpoint from a dict shaped like ckpt_load()'s (the predictor table empty)."""
+    L = lib()
+    L.sqb_ckpt_save.argtypes = [C.c_char_p, C.POINTER(Checkpoint)]
+    c = Checkpoint()
+    keep = []
+    for f, _ in Checkpoint._fields_:
+        if f in ('cur', 'nxt'):
+            a = np.ascontiguousarray(d[f], dtype=np.int8).reshape(-1)
+            keep.append(a)
+            setattr(c, f, a.ctypes.data_as(C.POINTER(C.c_byte)))
+        elif f == 'name':
+            c.name = d['name'].encode()
+        elif f == 'vs':
+            c.vs = None
+        elif f in ('Slev', 'S', 'es', 'cnt'):
+            arr = getattr(c, f)
+            for i, x in enumerate(d[f]):
+                arr[i] = x
+        elif f in d:
+            setattr(c, f, d[f])
+    c.vcap = 0
+    if L.sqb_ckpt_save(path.encode(), C.byref(c)):
+        raise SqbError('could not write %s' % path)
 
 
 def graphs():
@@ -110,13 +185,58 @@ def hsum(graph, h, N, eps, top=-1, **opts):
     o = default_opts(**opts)
     r = Result()
     rc = lib().sqb_hsum(graph.encode(), float(h), int(N), float(eps), int(top), C.byref(o), C.byref(r))
+    if rc == CKPT_STOPPED and opts.get('ckpt_stop'):
+        return None
     if rc:
         raise SqbError('%s: %s' % (graph, lib().sqb_error().decode()))
+    return _result_dict(r)
+
+
+def _result_dict(r):
     d = {f: getattr(r, f) for f, _ in Result._fields_}
     d['S'] = list(r.S)
     d['lev_evals'] = list(r.lev_evals)[:r.nlev]
     d['lev_ms'] = list(r.lev_ms)[:r.nlev]
     return d
+
+
+def _jobs(jobs):
+    """[(graph, h, N, eps[, top[, cost]])] -> a sqb_job_t array (top -1: the default)"""
+    arr = (Job * len(jobs))()
+    for i, j in enumerate(jobs):
+        g, h, N, eps = j[:4]
+        arr[i] = Job(g.encode(), float(h), int(N), float(eps), int(j[4]) if len(j) > 4 else -1,
+                     float(j[5]) if len(j) > 5 else 0.0)
+    return arr
+
+
+def hsum_batch(jobs, workers=4, **opts):
+    """Many integrals concurrently (sqb_hsum_batch): jobs = [(graph, h, N, eps[, top[, cost]])].
+    Returns (results in job order as hsum() dicts, device milliseconds of the whole batch)."""
+    arr = _jobs(jobs)
+    n = len(jobs)
+    res = (Result * max(1, n))()
+    rcs = (C.c_int * max(1, n))()
+    ms = C.c_double()
+    o = default_opts(**opts)
+    rc = lib().sqb_hsum_batch(arr, n, C.byref(o), int(workers), res, rcs, C.byref(ms))
+    if rc:
+        raise SqbError('batch: %d failed: %s' % (rc, lib().sqb_error().decode()))
+    return [_result_dict(res[i]) for i in range(n)], ms.value
+
+
+def batch_tune(jobs, candidates=(1, 2, 4, 6, 8), **opts):
+    """The batch tuner (sqb_batch_tune): runs the calibration jobs once per candidate worker count;
+    returns (best worker count, {count: points per second of device time})."""
+    arr = _jobs(jobs)
+    cand = (C.c_int * len(candidates))(*candidates)
+    rate = (C.c_double * len(candidates))()
+    best = C.c_int()
+    o = default_opts(**opts)
+    rc = lib().sqb_batch_tune(arr, len(jobs), C.byref(o), cand, len(candidates), rate, C.byref(best))
+    if rc:
+        raise SqbError('tune: %s' % lib().sqb_error().decode())
+    return best.value, {c: rate[i] for i, c in enumerate(candidates)}
 
 
 def select(selectors):
