@@ -69,6 +69,10 @@ typedef struct {
     const char *ckpt_dir;  /* SINCQED_CKPT_DIR (NULL: the current directory) */
     int ckpt_stop;         /* test hook: 1 = return SQB_CKPT_STOPPED right after the first checkpoint is written,
                               as a run killed there would stop */
+    int fma;               /* SQB_FMA: 1 (default) = the FP64 pass runs the graph's contracted kernel (multiplies
+                              and adds fused, as the reference's own CPU build compiles its double half);
+                              0 = the kernel that rounds every operation as written, bit for bit the reference's
+                              double half built with -ffp-contract=off */
 } sqb_opts_t;
 #define SQB_CKPT_STOPPED 2 /* sqb_hsum's return code under ckpt_stop */
 
@@ -128,8 +132,8 @@ const char *sqb_graph_volkov(const char *name);
 double sqb_graph_flops(const char *name, int ab);
 
 /* pointwise evaluation of the graph kernels on the device, for parity checks: n points sf[i*D + d]
- * (the Sinc variables), outputs f and the |.| sum; prec 0 = FP64 (ab: SQ_AB), 1 = double-double,
- * returned as (hi, lo) pairs in f2 and ab2 (2n entries each) */
+ * (the Sinc variables), outputs f and the |.| sum; prec 0 = FP64 (ab: SQ_AB), 2 = FP64 contracted,
+ * 1 = double-double, returned as (hi, lo) pairs in f2 and ab2 (2n entries each) */
 int  sqb_eval_points(const char *graph, long n, const double *sf, int prec, int ab, double *f, double *abs_);
 
 /* the device the library runs on ("off" before the first call) */

@@ -41,6 +41,8 @@ ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 # reference CPU code compiled without contraction; the double-double code uses explicit intrinsics.
 NVFLAGS = ARCH + ['-O3', '-lineinfo', '-fmad=false', '-std=c++17', '-Xcompiler', '-fPIC',
                   '-diag-suppress', '177,550', '-I' + CSRC, '-I' + INC]
+# the second unit of every graph: its FP64 kernel with contraction (fused multiply-adds), for the fast form
+NVFLAGS_FMA = [f if f != '-fmad=false' else '-fmad=true' for f in NVFLAGS]
 CXX = 'g++'   # the system compiler (an environment CXX may lack libgomp.spec)
 CXXFLAGS = ['-O2', '-fPIC', '-fopenmp', '-std=c++17', '-I' + CSRC, '-I' + INC, '-I/usr/local/cuda/include']
 
@@ -99,9 +101,13 @@ def generate(srcs):
         seen.add(name)
         tu = os.path.join(GEN, 'k_%s.cu' % name)
         text = '#include "sqkern.cuh"\n#include "%s"\n' % os.path.basename(cuh)
-        if not os.path.exists(tu) or open(tu).read() != text:
-            with open(tu, 'w') as f:
-                f.write(text)
+        # the contracted FP64 kernel: its own unit and namespace (sqkern.cuh, SQ_GRAPH)
+        tuf = os.path.join(GEN, 'kf_%s.cu' % name)
+        textf = '#define SQB_FMA_TU 1\n#define SQG_NS(n) sqgf_##n\n' + text
+        for path, t in ((tu, text), (tuf, textf)):
+            if not os.path.exists(path) or open(path).read() != t:
+                with open(path, 'w') as f:
+                    f.write(t)
         graphs.append((name, D, cuh, tu))
     return graphs
 
@@ -146,7 +152,7 @@ def count_flops(graphs):
     L = ['/* generated by sincfeyn_b200/build.py: algorithmic flop counter */',
          '#include <stdio.h>', '#include "sqcount.h"', 'long sq_flops, sq_trans;',
          '#define SQ_TABLE static const', '#define SQ_FUNC', '#define SQ_CHUNK', '#define SQ_CHUNK_DD', '#define RABS(x) sq_rabs(x)',
-         '#define SQ_EXP(x) sq_exp(x)', '#define SQ_LOG(x) sq_log(x)',
+         '#define SQ_EXP(x) sq_exp(x)', '#define SQ_LOG(x) sq_log(x)', '#define SQG_NS(n) sqg_##n',
          '#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX) \\',
          'static void count_##NAME(void){ sq_count sf[D], ab; for(int d = 0; d < D; d++) sf[d] = sq_count(0.7 + 0.37*d); \\',
          '  sq_flops = 0; sq_trans = 0; sqg_##NAME::K<sq_count, 1>::f_##NAME(sf, &ab); long a1 = sq_flops, t1 = sq_trans; \\',
@@ -194,6 +200,10 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
         o = os.path.join(OBJ, 'k_%s.o' % name)
         if _newer(o, [tu, cuh] + khdrs):
             jobs_list.append([NVCC] + NVFLAGS + ['-I' + GEN, '-c', tu, '-o', o])
+        of = os.path.join(OBJ, 'kf_%s.o' % name)
+        tuf = os.path.join(GEN, 'kf_%s.cu' % name)
+        if _newer(of, [tuf, cuh] + khdrs):
+            jobs_list.append([NVCC] + NVFLAGS_FMA + ['-I' + GEN, '-c', tuf, '-o', of])
     rt_o = os.path.join(OBJ, 'runtime.o')
     if _newer(rt_o, [os.path.join(CSRC, 'runtime.cu')] + hdrs):
         jobs_list.append([NVCC] + NVFLAGS + ['-Xcompiler', '-fopenmp', '-c', os.path.join(CSRC, 'runtime.cu'), '-o', rt_o])
@@ -221,7 +231,8 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     with cf.ThreadPoolExecutor(max_workers=n) as ex:
         for f in [ex.submit(_run, c) for c in jobs_list]:
             f.result()
-    objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o, bat_o, ck_o]
+    objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + \
+           [os.path.join(OBJ, 'kf_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o, bat_o, ck_o]
     if _newer(LIBSO, objs):
         _run([NVCC] + ARCH + ['-shared', '-o', LIBSO] + objs + ['-Xcompiler', '-fopenmp', '-lgomp', '-lpthread'])
     main_cpp = os.path.join(CSRC, 'main.cpp')

@@ -78,7 +78,8 @@ class KernelSource:
 
 
 def emit(src):
-    """Header text for one graph: namespace sqg_<name> with the tables and two copies of the class
+    """Header text for one graph: namespace SQG_NS(<name>) (a macro of the including unit, normally
+    sqg_<name>) with the tables and two copies of the class
     template -- K, whose chunk functions are SQ_CHUNK (the FP64 evaluation: inlined, so that their
     argument arrays stay in registers), and KD, whose chunk functions are SQ_CHUNK_DD (double-double:
     real calls, which keeps the compile of the large kernels bounded) -- then SQ_GRAPH(...), which the
@@ -86,7 +87,7 @@ def emit(src):
     k = KernelSource(src)
     out = ['/* generated by sincfeyn_b200/codegen/kgen.py from %s (QREAL half, arithmetic unchanged) */'
            % re.sub(r'^.*?(kernels/)', r'\1', src),
-           'namespace sqg_%s {' % k.name]
+           'namespace SQG_NS(%s) {' % k.name]
     for name, n, vals in k.gl:
         out.append('SQ_TABLE double %s[%d] = {%s};' % (name, n, vals))
     out += ['#define REAL SqReal_', '#define FN(x) x',

@@ -48,6 +48,7 @@ extern "C" void sqb_default_opts(sqb_opts_t *o){
     o->abserr0 = 1e-15; o->abrel = 1e-3; o->nearf = 1e-3; o->ddslack = 1;
     o->abskip = 1; o->abcheck = 0; o->dropunres = 1; o->growskip = 2;
     o->alldd = 0; o->device = 0; o->max_children = 0; o->verbose = 0;
+    o->fma = 1;
 }
 
 extern "C" int sqb_graph_count(void){ return sqb_ngraphs(); }
@@ -77,6 +78,7 @@ struct Run {
 static void set_test(Run &R, double abserr){
     R.t.abserr = abserr; R.t.nearf = R.o.nearf; R.t.ddslack = R.o.ddslack;
     R.t.abskip = R.o.abskip; R.t.abcheck = R.o.abcheck; R.t.dropunres = R.o.dropunres; R.t.alldd = R.o.alldd;
+    R.t.fma = R.o.fma;
 }
 
 static int eval(Run &R, const std::vector<sqb_pt_t> &p, const unsigned char *skip, std::vector<double> &v, std::vector<unsigned char> &nr){
@@ -204,8 +206,8 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
     sqb_pt_t *dcur = NULL; long ncur = 0;
     double Slev[16]; int nl = 0; int esok, lev0 = top - 1; long cnext = 0;
     sqb_acc_t acc0; memset(&acc0, 0, sizeof acc0);
-    for(int i = 0; i < 3; i++) res->S[i] = NAN;
     if(resumed){
+        for(int i = 0; i < 3; i++) res->S[i] = NAN;
         res->nev = ck.nev; res->ref = ck.ref; res->prune = ck.prune; res->trunc = ck.trunc; res->kept_top = ck.kept_top;
         R.nq = ck.nq; res->abskipped = ck.cnt[1];
         nl = ck.nl; for(int i = 0; i < nl; i++) Slev[i] = ck.Slev[i];
@@ -232,6 +234,7 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
         if(top == 0 && go.gshn) res->prune = fabs(go.gshs);
         if(go.A == 0){ sqb_dev_free(dcur); res->t = now() - t0; res->nq = R.nq; res->unresdrop = R.unresdrop; return 0; }
         { double r = go.e2 > 0 ? go.e1/go.e2 : 0; res->trunc = (r > 0 && r < 1) ? go.e1*r/(1 - r) : go.e1; }
+        for(int i = 0; i < 3; i++) res->S[i] = NAN;
         Slev[nl++] = go.S;
         res->kept_top = ncur;
         res->t_top = now() - t0;

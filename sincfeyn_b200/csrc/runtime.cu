@@ -139,6 +139,12 @@ static int reserve_points(long n){
     return 0;
 }
 
+/* the FP64 kernel to run: the contracted one (which 2) when asked for and built, else the exact one */
+static inline int f64_which(const sqb_graph_t *g, int fma){ return fma && g->f64_fma ? 2 : 0; }
+static inline void launch_f64(const sqb_graph_t *g, int which, const sqb_eval_t *a, int grid, size_t smem, cudaStream_t s){
+    if(which == 2) g->f64_fma(a, grid, 128, smem, s); else g->f64(a, grid, 128, smem, s);
+}
+
 static int grid_for(const sqb_graph_t *g, int which, long npts, size_t smem){
     sqb_kattr_t at; int per = 2;
     if(g->attr(which, 128, smem, &at) && at.blocks_per_sm > 0) per = at.blocks_per_sm;
@@ -168,7 +174,8 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
     }
     CKR(cudaMemsetAsync(G.nfb, 0, sizeof(unsigned long long), G.s));
     if(KTIME) CKR(cudaEventRecord(G.k0, G.s));
-    g->f64(a, grid_for(g, 0, npts, smem), 128, smem, G.s);
+    const int w = f64_which(g, t->fma);
+    launch_f64(g, w, a, grid_for(g, w, npts, smem), smem, G.s);
     CKR(cudaGetLastError());
     if(KTIME) CKR(cudaEventRecord(G.k1, G.s));
     d.list = G.fb; d.nlist = G.nfb; d.listcap = G.cap; d.all = 0;
@@ -273,7 +280,7 @@ extern "C" int sqb_preload(const char *graph){
         const sqb_graph_t *g = SQB_ALL[i];
         if(graph && strcmp(graph, g->name)) continue;
         sqb_kattr_t at;
-        for(int which = 0; which < 2; which++) if(g->attr(which, 128, 4096, &at)) n++;
+        for(int which = 0; which < 3; which++) if(g->attr(which, 128, 4096, &at)) n++;
     }
     return n;
 }
@@ -632,11 +639,14 @@ extern "C" int sqb_eval_points_impl(const sqb_graph_t *g, long n, const double *
     a.pts = NULL; a.n = n; a.esize = 1; a.stride = D; a.flag_at = -1; a.cells = 0;
     a.X = dX; a.Wt = dX; a.K = 0; a.raw = 1; a.skip = dsk; a.v = dv; a.ab = dab; a.sfin = dsf; a.vlo = dvl; a.ablo = dabl;
     size_t smem = 2*sizeof(double);
-    if(prec == 0) g->f64(&a, grid_for(g, 0, n, smem), 128, smem, G.s);
-    else { sqb_dd_t d; memset(&d, 0, sizeof d); d.e = a; d.all = 1; d.uu = dvl; g->dd(&d, grid_for(g, 1, n, smem), 128, smem, G.s); }
+    if(prec == 0 || prec == 2){
+        const int w = f64_which(g, prec == 2);
+        if(prec == 2 && w != 2){ snprintf(g_err, sizeof g_err, "%s: no contracted FP64 kernel in this library", g->name); return -1; }
+        launch_f64(g, w, &a, grid_for(g, w, n, smem), smem, G.s);
+    } else { sqb_dd_t d; memset(&d, 0, sizeof d); d.e = a; d.all = 1; d.uu = dvl; g->dd(&d, grid_for(g, 1, n, smem), 128, smem, G.s); }
     CKR(cudaGetLastError());
     CKR(cudaStreamSynchronize(G.s));
-    if(prec == 0){
+    if(prec == 0 || prec == 2){
         CKR(cudaMemcpy(f, dv, n*sizeof(double), cudaMemcpyDeviceToHost));
         CKR(cudaMemcpy(abs_, dab, n*sizeof(double), cudaMemcpyDeviceToHost));
     } else {

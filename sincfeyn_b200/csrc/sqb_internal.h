@@ -64,8 +64,12 @@ typedef struct {
     int zlattice;                              /* 1: the variable is z itself (synthetic integrand) */
     void (*f64)(const sqb_eval_t *a, int grid, int block, size_t smem, void *stream);
     void (*dd)(const sqb_dd_t *a, int grid, int block, size_t smem, void *stream);
-    /* which: 0 FP64 kernel, 1 dd kernel; blocks_per_sm for this block size and dynamic shared memory */
+    /* which: 0 FP64 kernel, 1 dd kernel, 2 contracted FP64 kernel; blocks_per_sm for this block size and
+     * dynamic shared memory; 0 if that kernel is not in the library */
     int (*attr)(int which, int block, size_t smem, sqb_kattr_t *out);
+    /* the FP64 kernel compiled with contraction (-fmad=true: fused multiply-adds), from the graph's second
+     * translation unit; NULL if the library was built without it */
+    void (*f64_fma)(const sqb_eval_t *a, int grid, int block, size_t smem, void *stream);
 } sqb_graph_t;
 
 #ifdef __cplusplus

@@ -16,6 +16,7 @@ typedef struct {
     double abserr, nearf, ddslack;
     int abskip, abcheck, dropunres;
     int alldd;                        /* every point in double-double (the plain all-dd form) */
+    int fma;                          /* FP64 pass: the contracted kernel (fused multiply-adds) when present */
 } sqb_test_t;
 
 /* level accumulators, double-double (hi, lo) pairs */

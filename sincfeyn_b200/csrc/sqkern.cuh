@@ -20,6 +20,9 @@
 #include "sqdd.cuh"
 #include "sqb_internal.h"
 
+#ifndef SQG_NS
+#define SQG_NS(n) sqg_##n                    /* the graph's namespace (sqgf_<name> in the contracted unit) */
+#endif
 #define SQ_TABLE static __constant__ const
 #define SQ_FUNC __device__
 #define SQ_CHUNK __device__ __forceinline__      /* FP64: chunk arguments stay in registers */
@@ -157,9 +160,35 @@ __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_dd(const sqb_dd_t a){
 }
 
 /* SQ_GRAPH(name, volkov, L, D, weight, n, fixed): the generated file ends with it, after namespace
- * sqg_<name> with the class template K<Real, SQ_AB> holding f_<name>. */
+ * SQG_NS(name) with the class template K<Real, SQ_AB> holding f_<name>.
+ *
+ * Every graph has two translation units.  The first (compiled with -fmad=false) holds the FP64 kernel
+ * whose roundings are those of the source, the double-double kernel and the registry entry SQB_<name>.
+ * The second (SQB_FMA_TU, compiled with -fmad=true, namespace sqgf_<name> so that no symbol is shared)
+ * holds only the FP64 kernel with multiplies and adds contracted into fused multiply-adds, exported as
+ * SQB_<name>_f64fma and SQB_<name>_attrfma; the registry entry refers to them weakly. */
+#if defined(SQB_FMA_TU)
 #define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
-namespace sqg_##NAME {                                                                             \
+namespace SQG_NS(NAME) {                                                                           \
+struct F {                                                                                         \
+    template<class R, int AB> static __device__ __forceinline__ R f(const R *sf, R *ab){           \
+        return K<R, AB>::f_##NAME(sf, ab); }                                                       \
+};                                                                                                 \
+}                                                                                                  \
+extern "C" void SQB_##NAME##_f64fma(const sqb_eval_t *a, int grid, int block, size_t smem, void *st){ \
+    sqb_k_f64<SQG_NS(NAME)::F, D><<<grid, block, smem, (cudaStream_t)st>>>(*a); }                  \
+extern "C" int SQB_##NAME##_attrfma(int block, size_t smem, sqb_kattr_t *o){                       \
+    cudaFuncAttributes fa; int nb = 0;                                                             \
+    if(cudaFuncGetAttributes(&fa, sqb_k_f64<SQG_NS(NAME)::F, D>) != cudaSuccess) return 0;         \
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sqb_k_f64<SQG_NS(NAME)::F, D>, block, smem) \
+       != cudaSuccess) return 0;                                                                   \
+    o->regs = fa.numRegs; o->local_bytes = (int)fa.localSizeBytes;                                 \
+    o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; return 1; }
+#else
+#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
+extern "C" void SQB_##NAME##_f64fma(const sqb_eval_t *, int, int, size_t, void *) __attribute__((weak)); \
+extern "C" int SQB_##NAME##_attrfma(int, size_t, sqb_kattr_t *) __attribute__((weak));             \
+namespace SQG_NS(NAME) {                                                                           \
 struct F {                                                                                         \
     template<class R, int AB> static __device__ __forceinline__ R f(const R *sf, R *ab){           \
         return K<R, AB>::f_##NAME(sf, ab); }                                                       \
@@ -171,6 +200,7 @@ static void f64(const sqb_eval_t *a, int grid, int block, size_t smem, void *st)
 static void dd(const sqb_dd_t *a, int grid, int block, size_t smem, void *st){                     \
     sqb_k_dd<F, D><<<grid, block, smem, (cudaStream_t)st>>>(*a); }                                 \
 static int attr(int which, int block, size_t smem, sqb_kattr_t *o){                                \
+    if(which == 2) return SQB_##NAME##_attrfma ? SQB_##NAME##_attrfma(block, smem, o) : 0;          \
     cudaFuncAttributes fa; int nb = 0;                                                             \
     cudaError_t e = which ? cudaFuncGetAttributes(&fa, sqb_k_dd<F, D>)                             \
                           : cudaFuncGetAttributes(&fa, sqb_k_f64<F, D>);                           \
@@ -182,4 +212,5 @@ static int attr(int which, int block, size_t smem, sqb_kattr_t *o){             
     o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; return 1; }                     \
 }                                                                                                  \
 extern "C" const sqb_graph_t SQB_##NAME = {#NAME, VOLKOV, L, D, W, NP, FIX, 0,                     \
-    sqg_##NAME::f64, sqg_##NAME::dd, sqg_##NAME::attr};
+    SQG_NS(NAME)::f64, SQG_NS(NAME)::dd, SQG_NS(NAME)::attr, SQB_##NAME##_f64fma};
+#endif

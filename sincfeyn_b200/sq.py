@@ -23,7 +23,7 @@ class Opts(C.Structure):
     _fields_ = [('abserr0', C.c_double), ('abrel', C.c_double), ('nearf', C.c_double), ('ddslack', C.c_double),
                 ('abskip', C.c_int), ('abcheck', C.c_int), ('dropunres', C.c_int), ('growskip', C.c_int),
                 ('alldd', C.c_int), ('device', C.c_int), ('max_children', C.c_long), ('verbose', C.c_int),
-                ('ckpt_every', C.c_double), ('ckpt_dir', C.c_char_p), ('ckpt_stop', C.c_int)]
+                ('ckpt_every', C.c_double), ('ckpt_dir', C.c_char_p), ('ckpt_stop', C.c_int), ('fma', C.c_int)]
 
 
 class Result(C.Structure):
@@ -280,11 +280,12 @@ def run(h, N, eps, selectors, top=-1, **opts):
 
 
 def eval_points(graph, sf, prec=0, ab=1):
-    """The graph kernel at the points sf (n x D) on the device.  prec 0: FP64 (f, ab) arrays; prec 1:
+    """The graph kernel at the points sf (n x D) on the device.  prec 0: FP64 (f, ab) arrays, every
+    operation rounded as written; prec 2: FP64 with contraction (fused multiply-adds); prec 1:
     double-double, (f, ab) as (n, 2) arrays of (hi, lo)."""
     sf = np.ascontiguousarray(sf, dtype=np.float64)
     n = sf.shape[0]
-    if prec == 0:
+    if prec in (0, 2):
         f = np.empty(n)
         a = np.empty(n)
     else:
