@@ -5,19 +5,22 @@ fallback on the device.  Metric: integrand points per second and time-to-sum.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-A step is one integral's whole hierarchical sum through the public C ABI (sqb_hsum): the top-level
-grow and dilation, then every refinement level on the device.  The timed steps walk the set in a fixed
-order (registry order); K defaults to the whole set, so the timed region is the set's time-to-sum.
-The W warm-up steps run the first W integrals untimed.  With N ranks (torchrun) the integrals are dealt
-round-robin to the ranks (strong scaling, no collective on the data path); the time is the maximum
-over ranks.
+A step is one integral's whole hierarchical sum through the public C ABI: the top-level grow and
+dilation, then every refinement level on the device.  K defaults to the whole set; the timed region is
+the K integrals as one concurrent batch (sqb_hsum_batch, worker count from the batch tuner), so its
+device time is the set's time-to-sum.  The same integrals then run one at a time, each kernel timed
+alone, for the level-pass throughput and the FP64 roofline.  The W warm-up steps run the first W
+integrals untimed, then the tuner runs every 4th integral once per candidate worker count.  With N ranks
+(torchrun) the integrals are dealt round-robin to the ranks (strong scaling, no collective on the data
+path); the time is the maximum over ranks.
 
 JSON line (rank 0):
   value      points/s of the device-resident refinement levels: evaluated children / device time of the
              level passes (cell lists already in HBM when each pass starts; CUDA events on the library's
              stream)
-  e2e        points/s through sqb_hsum with host-side parameters and host-side results, every host<->device
-             copy inside (all evaluated points / device-timed steps); time_to_sum_s is the set's total
+  e2e        points/s through sqb_hsum_batch with host-side parameters and host-side results, every
+             host<->device copy inside (all evaluated points / device time of the batch); time_to_sum_s
+             is that device time; one_at_a_time the same integrals through sqb_hsum one after another
   roofline   the FP64 evaluation kernels (sqb_k_f64<graph>): algorithmic flops per point (+ - * / of the
              kernel's double path, counted by the code generator; skipped |.| sums counted as skipped) over
              their event-timed launches, against this device's FP64 FMA rate measured by a probe kernel
@@ -25,6 +28,14 @@ JSON line (rank 0):
              bounded sample of the same workload
   vs_alldd   the same sample of integrals in the plain all-double-double form, time ratio
 `--impl reference` times the reference CPU build on the same metric (rank 0 only).
+
+Other measurements (one GPU, each prints its own JSON lines; not the headline):
+  --workload mixed   all2 + all3 at h = 1.0, 0.9, 0.8, 0.7 (184 integrals): one at a time against the
+                     tuned concurrent batch (sqb_hsum_batch), results compared
+  --workload synth   the synthetic Sinc-sum microbenchmark (d = 5, 8, 11; h = 1.0, 0.7) and its
+                     precision table (FP64 only, FP64 + dd, all-dd, the reference's hsum)
+  --workload vp4     the four-loop lepton-loop set (kernels/v4, kernels/w4) at h = 1.0 and 0.9, with the
+                     exactly known set values
 """
 import argparse
 import json
@@ -45,6 +56,7 @@ SET = 'all3'
 CPU_SAMPLE = ['g3_07', 'v3_01', 'g3_01']
 ALLDD_SAMPLE = ['v3_01', 'g3_07', 'g3_01']
 PROFILE_TRAFFIC = os.path.join(ROOT, 'profiles', 'fp64_kernel_traffic.json')
+BATCH_CANDIDATES = (2, 4, 8)     # worker streams tried by the batch tuner
 
 
 def env_rank():
@@ -201,6 +213,51 @@ def run_mixed(args, sq, L):
     print(json.dumps(line), flush=True)
 
 
+# the lepton-loop sets with exactly known values (docs/LEPTON_LOOPS.md:5-17; Laporta, Table 2)
+VP4_SETS = [('I(a) Pi2^3', lambda n: n == 'v4_00', 0.000876865858890),
+            ('I(b) Pi2+Pi4', lambda n: n.startswith('w4_00'), 0.015325282902013),
+            ('I(c) Pi4 with Pi2 inside', lambda n: n.startswith('w4_0i'), 0.011130913987517),
+            ('II(a) Pi4 in 2-loop vertices', lambda n: n[:5] in ('w4_01', 'w4_02', 'w4_03', 'w4_04', 'w4_05',
+                                                               'w4_06', 'w4_07'), -0.420482262508962),
+            ('II(b)+II(c)+III Pi2 insertions', lambda n: n.startswith('v4_') and n != 'v4_00', -0.027675 - 0.073452 + 1.417687)]
+VP4_H = ((1.0, 97), (0.9, 107))
+
+
+def run_vp4(args, sq, L):
+    """--workload vp4: the four-loop lepton-loop kernels (kernels/v4, kernels/w4: 118 integrals, D = 6..9)
+    at h = 1.0 (N = 97) and 0.9 (N = 107), eps = 1e-12, as one concurrent batch per h; the device time,
+    points/s, and each lepton-loop set's sum against its exact value."""
+    import torch
+    names = sq.select(['vp4'])
+    info = {g['name']: g for g in sq.graphs()}
+    for g in names:
+        sq.preload(g)
+    workers = args.workers or 6
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    out = []
+    for h, N in VP4_H:
+        if args.vp4_h and h not in args.vp4_h:
+            continue
+        jobs = [(g, h, N, EPS, -1, (2.0/h)**info[g]['D']) for g in names]
+        res, ms = sq.hsum_batch(jobs, workers=workers)
+        nev = sum(r['nev'] for r in res)
+        val = {g: r['S'][0]*info[g]['weight'] for g, r in zip(names, res)}
+        sets = []
+        for label, pick, exact in VP4_SETS:
+            mem = [g for g in names if pick(g)]
+            s = sum(val[g] for g in mem)
+            sets.append({'set': label, 'graphs': len(mem), 'sum': s, 'exact': exact, 'diff': s - exact})
+        slow = sorted(zip(names, res), key=lambda x: -x[1]['t'])[:5]
+        row = {'h': h, 'N': N, 'integrals': len(jobs), 'workers': workers, 'device_s': ms*1e-3, 'points': nev,
+               'points_s': nev/(ms*1e-3), 'fallback': sum(r['nq'] for r in res), 'sets': sets,
+               'slowest': [[g, round(r['t'], 2), r['nev']] for g, r in slow],
+               'values': {g: val[g] for g in names}}
+        out.append(row)
+        print(json.dumps(row), flush=True)
+    print(json.dumps({'workload': 'vp4', 'clocks': clocks.stop(), 'cases': len(out)}), flush=True)
+
+
 SYN_D = (5, 8, 11)
 SYN_H = (1.0, 0.7)
 GOLDEN_SYNTH = os.path.join(ROOT, 'tests', 'golden', 'synth_runs.json')
@@ -211,7 +268,7 @@ def run_synth(args, sq, L):
     """--workload synth: the synthetic Sinc-sum microbenchmark (d = 5, 8, 11; h = 1.0, 0.7; N =
     2 ceil(30/h) + 1; eps = 1e-12).  Per case: points/s and FP64 rate of the FP64+dd form, and the
     precision table: the value in FP64 only (no fallback: the fallback bound set to infinity), FP64+dd,
-    all double-double (d <= 8), against the reference's hsum() on the host-double-double oracle build
+    all double-double (not d = 11 at h = 1.0), against the reference's hsum() on the host-double-double oracle build
     where a golden run exists (d = 5 both h, d = 8 at h = 1.0)."""
     import torch
     with open(FLOPS_JSON) as f:
@@ -236,7 +293,7 @@ def run_synth(args, sq, L):
             N = 2*math.ceil(30/h - 1e-9) + 1
             row = {'d': d, 'h': h, 'N': N}
             for form, kw in (('fp64dd', {}), ('fp64', {'abserr0': 1e300}), ('alldd', {'alldd': 1})):
-                if form == 'alldd' and d > 8:
+                if form == 'alldd' and d > 8 and h > 0.8:      # d = 11 at h = 1.0: 4e11 points, minutes in dd
                     continue
                 L.sqb_timer_start()
                 r = sq.run(h, N, EPS, [name], **kw)[0]
@@ -275,9 +332,12 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-alldd', action='store_true', help='skip the all-double-double comparison')
-    ap.add_argument('--workload', default='all3', choices=['all3', 'mixed', 'synth'],
+    ap.add_argument('--workers', type=int, default=0, help='batch workers for --workload vp4 (default 6)')
+    ap.add_argument('--vp4-h', type=float, action='append', help='--workload vp4: only these h (repeatable)')
+    ap.add_argument('--workload', default='all3', choices=['all3', 'mixed', 'synth', 'vp4'],
                     help='all3: the headline line; mixed: the mixed batch, one-at-a-time vs concurrent; '
-                         'synth: the synthetic microbenchmark and its precision table (one GPU)')
+                         'synth: the synthetic microbenchmark and its precision table; vp4: the four-loop '
+                         'lepton-loop set at h=1.0 and 0.9 (one GPU)')
     args = ap.parse_args()
     rank, world, local = env_rank()
     if args.workload != 'all3':
@@ -287,7 +347,7 @@ def main():
             L = sq.lib()
             L.sqb_timer_stop.restype = C.c_double
             sq.kernel_timing(True)
-            (run_mixed if args.workload == 'mixed' else run_synth)(args, sq, L)
+            {'mixed': run_mixed, 'synth': run_synth, 'vp4': run_vp4}[args.workload](args, sq, L)
         return
     if world > 1:
         import torch.distributed as dist
@@ -310,6 +370,7 @@ def main():
     if args.steps is None:
         args.steps = len(names)
     order = [names[i % len(names)] for i in range(args.steps)]
+    D_OF = {x['name']: x['D'] for x in sq.graphs()}
     mine = assign(order, rank, world)
     L = sq.lib()
     import ctypes as C
@@ -322,9 +383,13 @@ def main():
     for g in names:
         sq.preload(g)
     t_load = time.perf_counter() - t_load
-    # warm-up: the first W integrals of the set, untimed
+    # warm-up: the first W integrals of the set, untimed; then the batch tuner on every 4th integral of
+    # this rank's share (it also warms the worker threads' buffers)
     for g in names[:args.warmup]:
         sq.hsum(g, H, N_PTS, EPS, device=local)
+    # cost estimate for the largest-first order: children per cell times flops per point
+    jobs = [(g, H, N_PTS, EPS, -1, float(2**D_OF[g])*sq.flops(g, 1)) for g in mine]
+    workers, tune_rates = sq.batch_tune(jobs[::4], BATCH_CANDIDATES, device=local)
     peak = sq.probe_fp64(True)
     flops = {g: (sq.flops(g, 1), sq.flops(g, 0)) for g in names}
     weight = {x['name']: x['weight'] for x in sq.graphs()}
@@ -335,8 +400,19 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
+    # the timed region: this rank's integrals as one concurrent batch (sqb_hsum_batch), device time
+    L.sqb_l2_flush(256 << 20)
     t_wall = time.perf_counter()
-    step_ms, lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches, results = 0.0, 0.0, 0, 0, 0.0, 0, 0.0, 0, []
+    bres, batch_ms = sq.hsum_batch(jobs, workers=workers, device=local)
+    wall = time.perf_counter() - t_wall
+    h1 = (C.c_ulonglong(), C.c_ulonglong())
+    L.sqb_copy_bytes(C.byref(h1[0]), C.byref(h1[1]))
+    nev = sum(r['nev'] for r in bres)
+    launches = sum(r['launches'] for r in bres)
+    bvals = {j[0]: r['S'][0] for j, r in zip(jobs, bres)}
+    # the same integrals one at a time, each kernel timed alone: the level-pass throughput and the FP64
+    # roofline (a kernel that shares the device with other streams would read slow)
+    step_ms, lev_ms, lev_ev, f64_ms, f64_n, fl, results, same = 0.0, 0.0, 0, 0.0, 0, 0.0, [], True
     for g in mine:
         L.sqb_l2_flush(256 << 20)
         L.sqb_timer_start()
@@ -345,23 +421,20 @@ def main():
         step_ms += ms
         lev_ms += sum(r['lev_ms'])
         lev_ev += sum(r['lev_evals'])
-        nev += r['nev']
         f64_ms += r['f64_ms']
         f64_n += r['f64_launches']
-        launches += r['launches'] + 1
         a1, a0 = flops[g]
         fl += (r['nev'] - r['abskipped'])*a1 + r['abskipped']*a0
+        same = same and (r['S'][0] == bvals[g] or (r['S'][0] != r['S'][0] and bvals[g] != bvals[g]))
         results.append([g, r['S'][0]*weight[g], r['nev'], r['nq'], round(ms, 2), round(1e3*r['t_top'], 2),
                         round(sum(r['lev_ms']), 2)])
     torch.cuda.synchronize()
-    wall = time.perf_counter() - t_wall
     clk = clocks.stop()
-    h1 = (C.c_ulonglong(), C.c_ulonglong())
-    L.sqb_copy_bytes(C.byref(h1[0]), C.byref(h1[1]))
-    mx, sm = reduce_max_sum([step_ms, wall], [lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches,
-                                              h1[0].value - h0[0].value, h1[1].value - h0[1].value], world)
-    step_ms, wall = mx
-    lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches, h2d, d2h = sm
+    mx, sm = reduce_max_sum([batch_ms, step_ms, wall], [lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches,
+                                                         h1[0].value - h0[0].value, h1[1].value - h0[1].value,
+                                                         0 if same else 1], world)
+    batch_ms, step_ms, wall = mx
+    lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches, h2d, d2h, ndiff = sm
     if rank != 0:
         if world > 1:
             import torch.distributed as dist
@@ -377,21 +450,26 @@ def main():
     line = {
         'metric': 'integrand points/s (time-to-sum) of the three-loop set at h=0.7',
         'value': lev_ev/(lev_ms*1e-3) if lev_ms > 0 else None, 'unit': 'points/s',
-        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': step_ms/max(1, len(mine)),
+        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': batch_ms/max(1, len(mine)),
         'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f64+dd',
         'data': 'the reference kernels (kernels/g3, kernels/v3) as integrands; no external data',
         'precision': 'FP64 pass contracted (fused multiply-adds), double-double fallback and level sums',
         'config': {'workload': '%s (%d integrals) h=%g N=%d eps=%g top=2, FP64 + double-double fallback'
                                % (SET, len(names), H, N_PTS, EPS),
-                   'integrals_timed': args.steps, 'l2': 'flushed (256 MiB memset) before every step',
+                   'integrals_timed': args.steps,
+                   'l2': 'flushed (256 MiB memset) before the batch and before every one-at-a-time integral',
                    'kernels': 'device code of the set\'s kernels loaded before the timed region (load_s %.2f s, once per process)' % t_load,
-                   'parallelism': 'integrals dealt round-robin over %d GPU(s)' % world},
-        'time_to_sum_s': step_ms*1e-3 if args.steps >= len(names) else None,
-        'e2e': {'value': nev/(step_ms*1e-3), 'unit': 'points/s', 'h2d_bytes_per_step': int(h2d/args.steps),
+                   'parallelism': 'integrals dealt round-robin over %d GPU(s); on each, one concurrent batch of %d worker streams'
+                                  % (world, workers)},
+        'time_to_sum_s': batch_ms*1e-3 if args.steps >= len(names) else None,
+        'e2e': {'value': nev/(batch_ms*1e-3), 'unit': 'points/s', 'h2d_bytes_per_step': int(h2d/args.steps),
                 'd2h_bytes_per_step': int(d2h/args.steps), 'wall_s': wall},
+        'batch': {'workers': workers, 'tuner_points_s': tune_rates, 'device_s': batch_ms*1e-3},
+        'one_at_a_time': {'device_s': step_ms*1e-3, 'points_s': nev/(step_ms*1e-3),
+                          'same_values_as_batch': ndiff == 0},
         'roofline': {'bound': 'fp64', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
                      'frac': achieved/peak if achieved else None, 'traffic': traffic,
-                     'kernel': 'sqb_k_f64<graph> (FP64 evaluation)',
+                     'kernel': 'sqb_k_f64<graph> (FP64 evaluation), timed one integral at a time',
                      'peak_source': 'measured FP64 FMA rate (probe kernel, this device)',
                      'flops_per_launch': fl/max(1, f64_n), 'launches': int(f64_n)},
         'gpu_launches': int(launches),

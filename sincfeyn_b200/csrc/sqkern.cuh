@@ -34,6 +34,9 @@
 #ifndef SQB_BLOCK
 #define SQB_BLOCK 128
 #endif
+#ifndef SQB_MINB
+#define SQB_MINB 1            /* FP64 kernel: resident blocks per SM the register allocation must allow */
+#endif
 #define SQB_QEPS 4.93e-32   /* double-double epsilon of the fallback's error model (driver/common.h:8) */
 
 /* coordinates and weight of point i; returns false for a child below the box */
@@ -89,7 +92,7 @@ __device__ __forceinline__ void sqb_tables(const sqb_eval_t &a, double *sX, doub
 }
 
 template<class F, int D>
-__global__ void __launch_bounds__(SQB_BLOCK) sqb_k_f64(const sqb_eval_t a){
+__global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const sqb_eval_t a){
     extern __shared__ double sqb_sm[];
     double *sX = sqb_sm, *sW = sqb_sm + (2*a.K + 1);
     sqb_tables(a, sX, sW);

@@ -21,14 +21,14 @@ GRAPHS = ['v4_00', 'w4_00Sc', 'v4_40', 'w4_01Sc']
 @pytest.mark.parametrize('name', GRAPHS)
 def test_four_loop_graph_matches_the_reference_run(name, fma):
     """as written (fma 0): the same evaluation count; contracted (fma 1, the default): point values move
-    by rounding, so points at the keep threshold may flip: counts within 1e-5"""
+    by rounding, so points at the keep threshold may flip: counts within 1e-4"""
     if name not in {g['name'] for g in sq.graphs()}:
         pytest.skip('%s not in this build' % name)
     rows, _ = refpy.run(refpy.SINCQED_EXACT, 1.0, 97, 1e-12, [name], top=1, env={'SINCQED_SYM': '0', 'SINCQED_KEEPBT': '1'})
     e = rows[0]
     r = sq.run(1.0, 97, 1e-12, [name], top=1, fma=fma)[0]
     if fma:
-        assert abs(r['evals'] - e['evals']) <= 1e-5*e['evals'], (name, r['evals'], e['evals'])
+        assert abs(r["evals"] - e["evals"]) <= 1e-4*e["evals"], (name, r["evals"], e["evals"])
     else:
         assert r['evals'] == e['evals'], (name, r['evals'], e['evals'])
     assert abs(r['value'] - e['value']) <= 1e-11*abs(e['value']) + 1e-18, (name, r['value'], e['value'])

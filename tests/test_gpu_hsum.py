@@ -66,7 +66,7 @@ def test_all2_contracted_form_agrees(rows_fast, golden):
     ref = {r['name']: r for r in golden['reference_exact_unfolded']}
     for r in rows_fast:
         e = ref[r['name']]
-        assert abs(r['evals'] - e['evals']) <= 1e-5*e['evals'], (r['name'], r['evals'], e['evals'])
+        assert abs(r['evals'] - e['evals']) <= 1e-4*e['evals'], (r['name'], r['evals'], e['evals'])
         assert abs(r['value'] - e['value']) <= 1e-13*abs(e['value']), (r['name'], r['value'], e['value'])
         assert abs(r['value'] - EXACT[r['name']]) < 2e-6
 
@@ -93,7 +93,7 @@ def test_three_loop_graphs_match_the_reference_run(name, fma):
     e = rows[0]
     r = sq.run(1.0, 97, 1e-12, [name], top=1, fma=fma)[0]
     if fma:
-        assert abs(r['evals'] - e['evals']) <= 1e-5*e['evals'], (name, r['evals'], e['evals'])
+        assert abs(r["evals"] - e["evals"]) <= 1e-4*e["evals"], (name, r["evals"], e["evals"])
     else:
         assert r['evals'] == e['evals'], (name, r['evals'], e['evals'])
     assert abs(r['value'] - e['value']) <= 1e-11*abs(e['value']) + 1e-15, (name, r['value'], e['value'])
