@@ -26,7 +26,8 @@ JSON line (rank 0):
              their event-timed launches, against this device's FP64 FMA rate measured by a probe kernel
   cpu_baseline  the reference's own OpenMP CPU build (oracle/_ref/sincqed) on this host's cores, on a
              bounded sample of the same workload
-  vs_alldd   the same sample of integrals in the plain all-double-double form, time ratio
+  vs_alldd   a sample of the set (or the whole set, --alldd-full) in the contracted, the as-written and the
+             plain all-double-double forms, one integral at a time: time ratio
 `--impl reference` times the reference CPU build on the same metric (rank 0 only).
 
 Other measurements (one GPU, each prints its own JSON lines; not the headline):
@@ -36,6 +37,8 @@ Other measurements (one GPU, each prints its own JSON lines; not the headline):
                      precision table (FP64 only, FP64 + dd, all-dd, the reference's hsum)
   --workload vp4     the four-loop lepton-loop set (kernels/v4, kernels/w4) at h = 1.0 and 0.9, with the
                      exactly known set values
+  --workload single  one integral (--graph) warm, then timed once: a small command for profilers
+  --workload points  one launch of a graph's evaluation kernel on --npoints seeded nodes (--prec)
 """
 import argparse
 import json
@@ -54,7 +57,7 @@ H, N_PTS, EPS = 0.7, 139, 1e-12
 SET = 'all3'
 # the CPU samples: three-loop integrals of D = 5, 5 and 6 at the workload's (h, N, eps)
 CPU_SAMPLE = ['g3_07', 'v3_01', 'g3_01']
-ALLDD_SAMPLE = ['v3_01', 'g3_07', 'g3_01']
+ALLDD_SAMPLE = ['v3_01', 'g3_07', 'g3_01', 'g3_00']
 PROFILE_TRAFFIC = os.path.join(ROOT, 'profiles', 'fp64_kernel_traffic.json')
 BATCH_CANDIDATES = (2, 4, 8)     # worker streams tried by the batch tuner
 
@@ -258,6 +261,28 @@ def run_vp4(args, sq, L):
     print(json.dumps({'workload': 'vp4', 'clocks': clocks.stop(), 'cases': len(out)}), flush=True)
 
 
+def run_single(args, sq, L):
+    """--workload single: one integral (--graph, at the headline's h, N, eps) once warm, then once timed; a
+    small, fixed command for profilers.  --workload points: one launch of the graph's FP64 kernel
+    (--prec 0 as written, 2 contracted) or double-double kernel (--prec 1) on --npoints seeded nodes."""
+    import numpy as np
+    g = args.graph
+    sq.preload(g)
+    if args.workload == 'points':
+        D = {x['name']: x['D'] for x in sq.graphs()}[g]
+        sf = np.exp(np.random.default_rng(1).uniform(-3, 3, size=(args.npoints, D)))
+        f, _ = sq.eval_points(g, sf, args.prec, 1)
+        print(json.dumps({'workload': 'points', 'graph': g, 'prec': args.prec, 'points': args.npoints,
+                          'sum_abs_f': float(np.nansum(np.abs(f if args.prec != 1 else f[:, 0])))}), flush=True)
+        return
+    sq.hsum(g, H, N_PTS, EPS)
+    L.sqb_timer_start()
+    r = sq.hsum(g, H, N_PTS, EPS)
+    ms = L.sqb_timer_stop()
+    print(json.dumps({'workload': 'single', 'graph': g, 'h': H, 'N': N_PTS, 'ms': ms, 'points': r['nev'],
+                      'f64_ms': r['f64_ms'], 'levels_ms': sum(r['lev_ms']), 'top_ms': 1e3*r['t_top']}), flush=True)
+
+
 SYN_D = (5, 8, 11)
 SYN_H = (1.0, 0.7)
 GOLDEN_SYNTH = os.path.join(ROOT, 'tests', 'golden', 'synth_runs.json')
@@ -332,9 +357,13 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-alldd', action='store_true', help='skip the all-double-double comparison')
+    ap.add_argument('--alldd-full', action='store_true', help='all-double-double comparison on the whole set (~2 min)')
     ap.add_argument('--workers', type=int, default=0, help='batch workers for --workload vp4 (default 6)')
     ap.add_argument('--vp4-h', type=float, action='append', help='--workload vp4: only these h (repeatable)')
-    ap.add_argument('--workload', default='all3', choices=['all3', 'mixed', 'synth', 'vp4'],
+    ap.add_argument('--graph', default='g3_00', help='--workload single/points: the graph')
+    ap.add_argument('--prec', type=int, default=2, help='--workload points: 0 FP64 as written, 2 contracted, 1 dd')
+    ap.add_argument('--npoints', type=int, default=1 << 22, help='--workload points: number of nodes')
+    ap.add_argument('--workload', default='all3', choices=['all3', 'mixed', 'synth', 'vp4', 'single', 'points'],
                     help='all3: the headline line; mixed: the mixed batch, one-at-a-time vs concurrent; '
                          'synth: the synthetic microbenchmark and its precision table; vp4: the four-loop '
                          'lepton-loop set at h=1.0 and 0.9 (one GPU)')
@@ -347,7 +376,8 @@ def main():
             L = sq.lib()
             L.sqb_timer_stop.restype = C.c_double
             sq.kernel_timing(True)
-            {'mixed': run_mixed, 'synth': run_synth, 'vp4': run_vp4}[args.workload](args, sq, L)
+            {'mixed': run_mixed, 'synth': run_synth, 'vp4': run_vp4, 'single': run_single,
+             'points': run_single}[args.workload](args, sq, L)
         return
     if world > 1:
         import torch.distributed as dist
@@ -486,13 +516,18 @@ def main():
         except Exception as e:                      # the oracle binary is test infrastructure; report why
             line['cpu_baseline'] = {'value': None, 'unavailable': str(e)[:200]}
     if world == 1 and not args.no_alldd:
-        t_f, t_x, t_d = 0.0, 0.0, 0.0
-        for g in ALLDD_SAMPLE:
-            L.sqb_timer_start(); sq.hsum(g, H, N_PTS, EPS); t_f += L.sqb_timer_stop()
-            L.sqb_timer_start(); sq.hsum(g, H, N_PTS, EPS, fma=0); t_x += L.sqb_timer_stop()
-            L.sqb_timer_start(); sq.hsum(g, H, N_PTS, EPS, alldd=1); t_d += L.sqb_timer_stop()
-        line['vs_alldd'] = {'sample': ALLDD_SAMPLE, 'fp64dd_s': t_f*1e-3, 'fp64dd_as_written_s': t_x*1e-3,
-                            'alldd_s': t_d*1e-3, 'speedup': t_d/t_f}
+        sample = names if args.alldd_full else ALLDD_SAMPLE
+        t = {}
+        for form, kw in (('fp64dd', {}), ('fp64dd_as_written', {'fma': 0}), ('alldd', {'alldd': 1})):
+            sq.hsum(sample[0], H, N_PTS, EPS, **kw)                 # warm: this form's kernels and buffers
+            t[form] = 0.0
+            for g in sample:
+                L.sqb_l2_flush(256 << 20)
+                L.sqb_timer_start(); sq.hsum(g, H, N_PTS, EPS, **kw); t[form] += L.sqb_timer_stop()*1e-3
+        line['vs_alldd'] = {'sample': 'all %d integrals' % len(sample) if args.alldd_full else sample,
+                            'fp64dd_s': t['fp64dd'], 'fp64dd_as_written_s': t['fp64dd_as_written'],
+                            'alldd_s': t['alldd'], 'speedup': t['alldd']/t['fp64dd'],
+                            'note': 'one integral at a time, each form warmed first, L2 flushed before each integral'}
     line['per_integral'] = {'columns': ['graph', 'value', 'evals', 'fallback', 'ms', 'top_ms', 'levels_ms'], 'rows': results}
     print(json.dumps(line), flush=True)
     if world > 1:

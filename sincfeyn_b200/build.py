@@ -151,7 +151,7 @@ def count_flops(graphs):
     exe = os.path.join(BUILD, 'count')
     L = ['/* generated by sincfeyn_b200/build.py: algorithmic flop counter */',
          '#include <stdio.h>', '#include "sqcount.h"', 'long sq_flops, sq_trans;',
-         '#define SQ_TABLE static const', '#define SQ_FUNC', '#define SQ_CHUNK', '#define SQ_CHUNK_DD', '#define RABS(x) sq_rabs(x)',
+         '#define SQ_TABLE static const', '#define SQ_FUNC', '#define SQ_FUNC_K', '#define SQ_CHUNK', '#define SQ_CHUNK_DD', '#define RABS(x) sq_rabs(x)',
          '#define SQ_EXP(x) sq_exp(x)', '#define SQ_LOG(x) sq_log(x)', '#define SQG_NS(n) sqg_##n',
          '#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX) \\',
          'static void count_##NAME(void){ sq_count sf[D], ab; for(int d = 0; d < D; d++) sf[d] = sq_count(0.7 + 0.37*d); \\',

@@ -63,15 +63,15 @@ class KernelSource:
     def chunk(self, fname):
         return re.match(r'(bk|ab)_', fname) is not None
 
-    def body(self, chunk_attr='SQ_CHUNK'):
+    def body(self, chunk_attr='SQ_CHUNK', func_attr='SQ_FUNC'):
         """The QREAL half with each function turned into a static member of the class template; the chunk
-        functions (bk_/ab_) get chunk_attr."""
+        functions (bk_/ab_) get chunk_attr, the others func_attr."""
         def repl(m):
             ret, fname = m.group(1), m.group(2)
-            attr = chunk_attr if self.chunk(fname) else 'SQ_FUNC'
+            attr = chunk_attr if self.chunk(fname) else func_attr
             return 'static %s %s FN(%s)(' % (attr, ret, fname)
         b = _FDEF.sub(repl, self.qhalf)
-        rest = re.sub(r'static (%s|SQ_FUNC)' % chunk_attr, '', b)
+        rest = re.sub(r'static (%s|%s)' % (chunk_attr, func_attr), '', b)
         if re.search(r'\bstatic\b', rest):
             raise ValueError('%s: unexpected static in the QREAL half' % self.path)
         return b
@@ -80,8 +80,8 @@ class KernelSource:
 def emit(src):
     """Header text for one graph: namespace SQG_NS(<name>) (a macro of the including unit, normally
     sqg_<name>) with the tables and two copies of the class
-    template -- K, whose chunk functions are SQ_CHUNK (the FP64 evaluation: inlined, so that their
-    argument arrays stay in registers), and KD, whose chunk functions are SQ_CHUNK_DD (double-double:
+    template -- K, whose chunk functions are SQ_CHUNK and whose other functions (pt_, vp_, helpers) are
+    SQ_FUNC_K (the FP64 evaluation: all inlined, so that the argument arrays stay in registers), and KD, whose chunk functions are SQ_CHUNK_DD (double-double:
     real calls, which keeps the compile of the large kernels bounded) -- then SQ_GRAPH(...), which the
     including translation unit defines (kernels and registry entry, or flop counter)."""
     k = KernelSource(src)
@@ -92,7 +92,7 @@ def emit(src):
         out.append('SQ_TABLE double %s[%d] = {%s};' % (name, n, vals))
     out += ['#define REAL SqReal_', '#define FN(x) x',
             'template<class SqReal_, int SQ_AB> struct K {',
-            k.body('SQ_CHUNK').strip('\n'),
+            k.body('SQ_CHUNK', 'SQ_FUNC_K').strip('\n'),
             '};']
     if any(k.chunk(f) for _, f in k.funcs):
         out += ['template<class SqReal_, int SQ_AB> struct KD {',

@@ -13,6 +13,10 @@
  * first launch; every worker records an end event after its last; the caller's stream waits on all of
  * them and records the stop event.  The elapsed time between start and stop is the batch's device time.
  *
+ * An integral that runs out of device memory beside the others (the grow's tables of a large four-loop
+ * integral at small h reach tens of GB) is not an error of the batch: it is run again after the queue
+ * is drained, alone on the device, by the calling thread.
+ *
  * The tuner runs a calibration list (normally a few integrals of the batch) once per candidate worker
  * count and returns the count with the highest evaluated points per second of device time. */
 #include <atomic>
@@ -43,7 +47,12 @@ struct Batch {
     std::vector<cudaEvent_t> ends;
     std::vector<int> ended;          /* worker recorded its end event */
     std::mutex m; std::condition_variable cv; int left = 0, failures = 0; std::string err;
+    std::vector<int> retry;          /* jobs that ran out of device memory: run again alone */
 };
+
+bool out_of_memory(const char *msg){
+    return strstr(msg, "out of memory") || strstr(msg, "allocation");
+}
 
 /* the pool: workers wait for a new generation.  Its mutex and condition variable are never destroyed:
  * the workers are detached and still wait on them when the process exits, and destroying a condition
@@ -70,8 +79,11 @@ void serve(Batch *b, int id){
         b->rcs[j] = sqb_hsum(J.graph, J.h, J.N, J.eps, J.top, &b->o, &b->res[j]);
         if(b->rcs[j]){
             std::lock_guard<std::mutex> lk(b->m);
-            b->failures++;
-            if(b->err.empty()) b->err = std::string(J.graph) + ": " + sqb_error();
+            if(out_of_memory(sqb_error())) b->retry.push_back(j);
+            else {
+                b->failures++;
+                if(b->err.empty()) b->err = std::string(J.graph) + ": " + sqb_error();
+            }
         }
     }
     int rec = ok && cudaEventRecord(b->ends[id], s) == cudaSuccess;
@@ -142,6 +154,17 @@ extern "C" int sqb_hsum_batch(const sqb_job_t *jobs, int n, const sqb_opts_t *o_
     }
     { std::lock_guard<std::mutex> lk(PM); CUR = nullptr; }
     for(int i = 0; i < workers; i++) if(b.ended[i]) cudaStreamWaitEvent(s, b.ends[i], 0);
+    if(!b.retry.empty()){
+        /* alone on the device now: every worker has finished, and its memory is back in the pool */
+        std::sort(b.retry.begin(), b.retry.end());
+        cudaStreamSynchronize(s);
+        for(int j : b.retry){
+            const sqb_job_t &J = jobs[j];
+            sqb_set_mem_share(1.0);
+            rcs[j] = sqb_hsum(J.graph, J.h, J.N, J.eps, J.top, &o, &res[j]);
+            if(rcs[j]){ b.failures++; if(b.err.empty()) b.err = std::string(J.graph) + ": " + sqb_error(); }
+        }
+    }
     cudaEvent_t stop = nullptr;
     if(cudaEventCreate(&stop) == cudaSuccess && cudaEventRecord(stop, s) == cudaSuccess && cudaEventSynchronize(stop) == cudaSuccess){
         float t = 0; cudaEventElapsedTime(&t, b.start, stop);

@@ -130,6 +130,9 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
     const int store = lev > 0, gs = lev == 0 && R.o.abskip ? R.o.growskip : 0;
     if(sqb_grow_begin(R.D, R.K, st, W, (const unsigned long long*)P, gs, R.o.abskip, sqb_dev_stream()))
         FAIL("device grow: %s", sqb_top_error());
+    /* the grow's device tables are released on every return, an error included, so that a failed
+     * integral leaves its memory to the next one */
+    struct End { ~End(){ sqb_grow_end(); } } end_of_grow;
     std::vector<double> v; std::vector<unsigned char> stt, cls;
     ksum ks; double a = 0, x1 = 0, x2 = 0, dr = 0, gshs = 0; long ne = 0, gshn = 0, nkeep = 0;
     for(;;){
@@ -163,7 +166,6 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
     if(sqb_grow_finish(thr, store && R.D < SQB_MAXD, &m)) FAIL("device grow: %s", sqb_top_error());
     *dilated = NULL; *ndil = 0;
     if(store && sqb_grow_dilate(nbits, dilated, ndil)) FAIL("device dilate: %s", sqb_top_error());
-    sqb_grow_end();
     go->S = ks.val(); go->A = a; go->e1 = x1; go->e2 = x2; go->drop = dr; go->gshs = gshs; go->gshn = gshn; go->nev = ne;
     return 0;
 }

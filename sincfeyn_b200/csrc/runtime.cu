@@ -48,7 +48,7 @@ extern "C" const sqb_graph_t *sqb_graph_at(int i){ return i >= 0 && i < SQB_NALL
 
 /* ------------------------------------------------------------------------------------------------ */
 #define RT 256                    /* threads per reduce / scatter CTA */
-#define RPT 16                    /* consecutive children per thread */
+#define RPT 16                    /* children per thread (scatter: consecutive; reduce: RT apart) */
 #define RTILE (RT*RPT)
 #define FT 1024                   /* threads of the one-CTA finish kernel (32 warps) */
 
@@ -304,14 +304,16 @@ __device__ __forceinline__ int parent_tier(const lvl_t &a, long i){
 
 /* per tile of RTILE children: S = sum v*pw and the shadow-tier sums in double-double per thread (they
  * can cancel), sum |v|, the dropped weight and the round column (non-negative) in double per thread,
- * then double-double across threads in a fixed tree */
+ * then double-double across threads in a fixed tree.  Thread t of the tile takes children t, t + RT,
+ * t + 2 RT, ... (each warp reads 256 contiguous bytes of v per step); the order is fixed, so a run is
+ * reproducible. */
 __global__ void __launch_bounds__(RT) sqb_k_reduce(const lvl_t a, part_t *bp, unsigned *bkeep){
-    const long t0 = blockIdx.x*(long)RTILE + threadIdx.x*(long)RPT;
+    const long t0 = blockIdx.x*(long)RTILE + threadIdx.x;
     sqdd S, b1, b2;
     double A = 0, dr = 0, uu = 0;
     unsigned ne = 0, nq = 0, nu = 0, nsk = 0, keep = 0;
     for(int j = 0; j < RPT; j++){
-        const long i = t0 + j;
+        const long i = t0 + (long)j*RT;
         if(i >= a.n) break;
         const unsigned char s = a.stt[i];
         if(!(s & SQB_PRESENT)) continue;

@@ -25,6 +25,10 @@
 #endif
 #define SQ_TABLE static __constant__ const
 #define SQ_FUNC __device__
+#ifndef SQ_FUNC_K
+#define SQ_FUNC_K __device__                    /* FP64 class: point functions (pt_, vp_, helpers); a graph's
+                                                   unit may define it __forceinline__ */
+#endif
 #define SQ_CHUNK __device__ __forceinline__      /* FP64: chunk arguments stay in registers */
 #define SQ_CHUNK_DD __device__ __noinline__     /* double-double: real calls bound the compile */
 #define RABS(x) sq_rabs(x)

@@ -26,6 +26,7 @@ SRC = r'''
 #include "sqdd.cuh"
 #define SQ_TABLE static const
 #define SQ_FUNC
+#define SQ_FUNC_K
 #define SQ_CHUNK
 #define SQ_CHUNK_DD
 #define RABS(x) sq_rabs(x)
