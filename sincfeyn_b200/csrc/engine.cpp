@@ -135,15 +135,18 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
     struct End { ~End(){ sqb_grow_end(); } } end_of_grow;
     std::vector<double> v; std::vector<unsigned char> stt, cls;
     ksum ks; double a = 0, x1 = 0, x2 = 0, dr = 0, gshs = 0; long ne = 0, gshn = 0, nkeep = 0;
+    double te = 0, th = 0, tx = 0; int nfr = 0; const double tg0 = now();    /* phase times (verbose) */
     for(;;){
         const sqb_pt_t *pts; const unsigned char *skip;
         const long n = sqb_grow_frontier(&pts, &skip);
         if(n <= 0) break;
         v.resize(n); stt.resize(n); cls.resize(n);
         const double *vd; const unsigned char *sd;
+        const double t0 = now();
         if(sqb_dev_eval_resident(R.g, pts, n, skip, &R.t, v.data(), stt.data(), &R.nq, &R.u, &R.unresdrop, &vd, &sd))
             FAIL("device: %s", sqb_last_error());
         if(sqb_grow_shells(cls.data())) FAIL("device grow: %s", sqb_top_error());
+        const double t1 = now(); te += t1 - t0; nfr++;
         ne += n;
         /* the frontier's sums in point order, then its threshold (driver/sumkey.h:225-245) */
         for(long i = 0; i < n; i++){ ks.add(v[i]*pw); a += fabs(v[i])*pw; }
@@ -154,9 +157,12 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
             if(!(fabs(v[i]) >= thr)){ dr += w; gshs += v[i]*pw; gshn++; }
         }
         long nk = 0, nn = 0;
+        const double t2 = now(); th += t2 - t1;
         if(sqb_grow_expand(vd, sd, thr, &nk, &nn)) FAIL("device grow: %s", sqb_top_error());
+        tx += now() - t2;
         nkeep += nk;
     }
+    const double tg1 = now();
     /* the final threshold, driver/sumkey.h:399-401 */
     const double thr = eps_rel*a;
     { std::vector<double> kv(nkeep);
@@ -164,8 +170,14 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
       for(long i = 0; i < nkeep; i++) if(!(kv[i] >= thr)) dr += kv[i]*pw; }
     long m = 0;
     if(sqb_grow_finish(thr, store && R.D < SQB_MAXD, &m)) FAIL("device grow: %s", sqb_top_error());
+    const double tg2 = now();
     *dilated = NULL; *ndil = 0;
     if(store && sqb_grow_dilate(nbits, dilated, ndil)) FAIL("device dilate: %s", sqb_top_error());
+    if(R.o.verbose)
+        fprintf(stderr, "# %s grow: %d frontiers, %ld points, %ld kept: eval %.1f ms, host sums %.1f ms, expand %.1f ms; "
+                "final threshold + tiers %.1f ms; dilate %.1f ms (%ld cells)\n", R.g->name, nfr, ne, nkeep,
+                1e3*te, 1e3*th, 1e3*tx, 1e3*(tg2 - tg1), 1e3*(now() - tg2), *ndil);
+    (void)tg0;
     go->S = ks.val(); go->A = a; go->e1 = x1; go->e2 = x2; go->drop = dr; go->gshs = gshs; go->gshn = gshn; go->nev = ne;
     return 0;
 }
