@@ -419,7 +419,10 @@ def main():
         sq.hsum(g, H, N_PTS, EPS, device=local)
     # cost estimate for the largest-first order: children per cell times flops per point
     jobs = [(g, H, N_PTS, EPS, -1, float(2**D_OF[g])*sq.flops(g, 1)) for g in mine]
-    workers, tune_rates = sq.batch_tune(jobs[::4], BATCH_CANDIDATES, device=local)
+    # the tuning sample leaves out the costliest integral: alone it sets the sample's time whatever the
+    # worker count, which would make the choice noise
+    top = max(j[5] for j in jobs)
+    workers, tune_rates = sq.batch_tune([j for j in jobs if j[5] < top][::4], BATCH_CANDIDATES, device=local)
     peak = sq.probe_fp64(True)
     flops = {g: (sq.flops(g, 1), sq.flops(g, 0)) for g in names}
     weight = {x['name']: x['weight'] for x in sq.graphs()}

@@ -66,6 +66,42 @@ def _run(cmd, log=None):
 
 
 SYNTH = os.path.join(PKG, 'synth')
+OCC = os.path.join(LIB, 'occupancy.json')
+
+# The contracted FP64 kernel's occupancy, chosen per graph at build time from the compiler's own report:
+# three resident CTAs per SM (registers capped at 168 for 128 threads) where that costs at most SPILL_MAX
+# bytes of spill stores, else the uncapped allocation.  Measured on the B200 at h = 0.7: the capped
+# kernels of the D = 7 three-loop graphs run 7-9 % faster, while g3_lbl, which would spill kilobytes,
+# runs slower capped.
+SPILL_MAX = 128
+_PTXAS_F64 = re.compile(r'Function properties for _Z9sqb_k_f64\S*\s*\n\s*(\d+) bytes stack frame, (\d+) bytes spill stores')
+
+
+def _compile_graph(tu, o, tuf, of, name, do_exact, do_fma):
+    """Both units of one graph.  A graph whose contracted kernel spills even at the uncapped allocation
+    (g3_lbl: ~1 KB of stack per thread) is built without the level-mode tile sums in both units: their
+    shared memory would take L1 from the stack it spills to (measured: g3_lbl 15 % slower with them)."""
+    info = None
+    if do_fma:
+        out = _run([NVCC] + NVFLAGS_FMA + ['-DSQB_MINB=3', '-Xptxas', '-v', '-I' + GEN, '-c', tuf, '-o', of])
+        m = _PTXAS_F64.search(out)
+        spill = int(m.group(2)) if m else -1
+        info = {'min_blocks': 3, 'spill_stores_at_3': spill, 'fused': 1}
+        if spill < 0 or spill > SPILL_MAX:
+            out = _run([NVCC] + NVFLAGS_FMA + ['-Xptxas', '-v', '-I' + GEN, '-c', tuf, '-o', of])
+            m = _PTXAS_F64.search(out)
+            spill1 = int(m.group(2)) if m else -1
+            info = {'min_blocks': 1, 'spill_stores_at_3': spill, 'spill_stores_at_1': spill1, 'fused': 1}
+            if spill1 < 0 or spill1 > SPILL_MAX:
+                _run([NVCC] + NVFLAGS_FMA + ['-DSQB_FUSE=0', '-I' + GEN, '-c', tuf, '-o', of])
+                info['fused'] = 0
+    elif os.path.exists(OCC):
+        with open(OCC) as f:
+            info = json.load(f).get(name)
+    if do_exact:
+        fuse = [] if not info or info.get('fused', 1) else ['-DSQB_FUSE=0']
+        _run([NVCC] + NVFLAGS + fuse + ['-I' + GEN, '-c', tu, '-o', o])
+    return name, info
 
 
 def kernel_sources(kdir, classes):
@@ -198,12 +234,12 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     jobs_list = []
     for name, D, cuh, tu in graphs:
         o = os.path.join(OBJ, 'k_%s.o' % name)
-        if _newer(o, [tu, cuh] + khdrs):
-            jobs_list.append([NVCC] + NVFLAGS + ['-I' + GEN, '-c', tu, '-o', o])
         of = os.path.join(OBJ, 'kf_%s.o' % name)
         tuf = os.path.join(GEN, 'kf_%s.cu' % name)
-        if _newer(of, [tuf, cuh] + khdrs):
-            jobs_list.append([NVCC] + NVFLAGS_FMA + ['-I' + GEN, '-c', tuf, '-o', of])
+        do_fma = _newer(of, [tuf, cuh] + khdrs + [os.path.abspath(__file__)])
+        do_exact = do_fma or _newer(o, [tu, cuh] + khdrs)
+        if do_fma or do_exact:
+            jobs_list.append(lambda a=(tu, o, tuf, of, name, do_exact, do_fma): _compile_graph(*a))
     rt_o = os.path.join(OBJ, 'runtime.o')
     if _newer(rt_o, [os.path.join(CSRC, 'runtime.cu')] + hdrs):
         jobs_list.append([NVCC] + NVFLAGS + ['-Xcompiler', '-fopenmp', '-c', os.path.join(CSRC, 'runtime.cu'), '-o', rt_o])
@@ -228,9 +264,17 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     n = jobs or min(len(jobs_list) or 1, os.cpu_count() or 4)
     if verbose and jobs_list:
         print('sincfeyn_b200: compiling %d objects with %d jobs' % (len(jobs_list), n), file=sys.stderr)
+    occ = {}
+    if os.path.exists(OCC):
+        with open(OCC) as f:
+            occ = json.load(f)
     with cf.ThreadPoolExecutor(max_workers=n) as ex:
-        for f in [ex.submit(_run, c) for c in jobs_list]:
-            f.result()
+        for f in [ex.submit(c) if callable(c) else ex.submit(_run, c) for c in jobs_list]:
+            r = f.result()
+            if isinstance(r, tuple) and r[1] is not None:
+                occ[r[0]] = r[1]
+    with open(OCC, 'w') as f:
+        json.dump(occ, f, indent=0, sort_keys=True)
     objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + \
            [os.path.join(OBJ, 'kf_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o, bat_o, ck_o]
     if _newer(LIBSO, objs):

@@ -77,6 +77,98 @@ class KernelSource:
         return b
 
 
+_PT_DEF = re.compile(r'^static REAL FN\((pt_\w+)\)\(const REAL \*x, const REAL Vx, REAL \*ab\)\{$', re.M)
+
+
+def split_plan(k, max_parts=6):
+    """A point function that is a flat sum of independent forest nodes can be evaluated in passes.
+
+    Returns None, or (groups, text) for the graph's FP64 split: the QREAL half's pt_<g> holds a header
+    (x0..x{n-1}), node sections (each opened by a `/* node` comment, using only the header and its own
+    names: checked), `REAL tot=0, tota=0;`, one accumulation block per node ending in `tot+=r` or
+    `tot-=r; tota+=ra; }`, and `*ab=tota; return tot;`; its f_<g> calls it once, from a one-point
+    Gauss-Legendre loop.  Pass P evaluates the nodes of group P and applies their accumulation blocks to
+    the running (tot, tota) of the point, kept in memory between passes; the final pass applies f_'s
+    own arithmetic to them.  Every operation and its order are those of the unsplit function, so the
+    values are the same.  The groups are consecutive nodes, about equal in text size."""
+    q = k.qhalf
+    m = _PT_DEF.search(q)
+    if not m:
+        return None
+    pt = m.group(1)
+    body_start = m.end()
+    end = q.index('\n}\n', body_start)
+    lines = q[body_start:end].split('\n')[1:]
+    heads = [n for n, l in enumerate(lines) if l.strip().startswith('/* node')]
+    tots = [n for n, l in enumerate(lines) if l.strip() == 'REAL tot=0, tota=0;']
+    if len(heads) < 8 or len(tots) != 1 or lines[-1].strip() != '*ab=tota; return tot;':
+        return None
+    header = lines[:heads[0]]
+    if not all(re.match(r'\s*const REAL x\d+=x\[\d+\];$', l) for l in header):
+        return None
+    secs = [lines[heads[a]:(heads[a + 1] if a + 1 < len(heads) else tots[0])] for a in range(len(heads))]
+    blocks, cur = [], []
+    for l in lines[tots[0] + 1:-1]:
+        cur.append(l)
+        if re.search(r'tot[+-]=r; tota\+=ra; \}$', l.strip()):
+            blocks.append(cur)
+            cur = []
+    if cur or len(blocks) != len(secs):
+        return None
+    defs = [set(re.findall(r'\b([A-Za-z_]\w*)(?=\[[^]]*\]*\s*(?:=|,|;))|(?:REAL|,)\s*([A-Za-z_]\w*)\s*[=;,\[]', '\n'.join(sec)))
+            for sec in secs]
+    names = [set(a or b for a, b in d) for d in defs]
+    hdr = set(re.findall(r'const REAL (x\d+)=', '\n'.join(header)))
+    for a, sec in enumerate(secs):
+        used = set(re.findall(r'\b([A-Za-z_]\w*)\b', '\n'.join(sec)))
+        for b, nb in enumerate(names):
+            if b != a and (used & (nb - names[a]) - hdr):
+                return None
+    # the f_ function: one call of pt, inside a one-point loop
+    fm = re.search(r'^static REAL FN\((f_%s)\)\(const REAL \*sf, REAL \*ab\)\{\n(.*?)\n\}$' % re.escape(k.name), q, re.M | re.S)
+    if not fm:
+        return None
+    fbody = fm.group(2)
+    call = 'FN(%s)(s,0,&a)' % pt
+    if fbody.count(call) != 1 or not re.search(r'for\(int g=0;g<1;g\+\+\)', fbody) or q.count('FN(%s)(' % pt) != 2:
+        return None
+    # consecutive groups of about equal text size
+    size = [sum(len(l) for l in sec) for sec in secs]
+    target = sum(size)/max_parts
+    groups, g, acc = [], [], 0
+    for a in range(len(secs)):
+        g.append(a); acc += size[a]
+        if acc >= target and len(groups) < max_parts - 1:
+            groups.append(g); g, acc = [], 0
+    if g:
+        groups.append(g)
+    out = []
+    for P, grp in enumerate(groups):
+        out.append('static SQ_FUNC_K void FN(ptp%d_%s)(const REAL *x, const REAL Vx, REAL *tot_, REAL *tota_){' % (P, k.name))
+        out += header
+        for a in grp:
+            out += secs[a]
+        out.append('  REAL tot=*tot_, tota=*tota_;')
+        for a in grp:
+            out += blocks[a]
+        out.append('  *tot_=tot; *tota_=tota;')
+        out.append('}')
+        fp = fbody.replace('REAL acc=0, aa=0, a;', '')
+        fp = fp.replace('const REAL wg=(REAL)GLW_%s[g]; acc+=wg*%s; aa+=wg*a; }' % (k.name, call),
+                        'FN(ptp%d_%s)(s,0,tot_,tota_); }' % (P, k.name))
+        fp = fp[:fp.index('const REAL nrm=')] if 'const REAL nrm=' in fp else None
+        if fp is None or 'FN(ptp' not in fp:
+            return None
+        out.append('static SQ_FUNC_K void FN(fpart%d_%s)(const REAL *sf, REAL *tot_, REAL *tota_){' % (P, k.name))
+        out.append(fp.rstrip())
+        out.append('}')
+    fin = fbody.replace(call, '(a=TA_, TT_)')
+    out.append('static SQ_FUNC_K REAL FN(ffin_%s)(const REAL *sf, const REAL TT_, const REAL TA_, REAL *ab){' % k.name)
+    out.append(fin)
+    out.append('}')
+    return groups, '\n'.join(out)
+
+
 def emit(src):
     """Header text for one graph: namespace SQG_NS(<name>) (a macro of the including unit, normally
     sqg_<name>) with the tables and two copies of the class
@@ -90,10 +182,16 @@ def emit(src):
            'namespace SQG_NS(%s) {' % k.name]
     for name, n, vals in k.gl:
         out.append('SQ_TABLE double %s[%d] = {%s};' % (name, n, vals))
+    plan = split_plan(k)
     out += ['#define REAL SqReal_', '#define FN(x) x',
             'template<class SqReal_, int SQ_AB> struct K {',
-            k.body('SQ_CHUNK', 'SQ_FUNC_K').strip('\n'),
-            '};']
+            k.body('SQ_CHUNK', 'SQ_FUNC_K').strip('\n')]
+    if plan:
+        out += ['/* the same point function in %d passes over groups of its nodes (kgen.split_plan) */' % len(plan[0]),
+                plan[1]]
+    out += ['};']
+    if plan:
+        out.append('#define SQ_SPLIT_%s %d' % (k.name, len(plan[0])))
     if any(k.chunk(f) for _, f in k.funcs):
         out += ['template<class SqReal_, int SQ_AB> struct KD {',
                 k.body('SQ_CHUNK_DD').strip('\n'),

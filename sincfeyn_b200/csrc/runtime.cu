@@ -52,10 +52,8 @@ extern "C" const sqb_graph_t *sqb_graph_at(int i){ return i >= 0 && i < SQB_NALL
 #define RTILE (RT*RPT)
 #define FT 1024                   /* threads of the one-CTA finish kernel (32 warps) */
 
-typedef struct {
-    double S[2], A[2], drop[2], b1[2], b2[2], u[2];
-    unsigned long long ne, nq, unres, skipped;
-} part_t;
+typedef sqb_part_t part_t;
+static_assert(RTILE == SQB_TILE, "the reduce kernel's tiles are the FP64 kernel's");
 
 typedef struct {
     const signed char *cells;     /* device pt_t list (12 bytes per cell) */
@@ -78,7 +76,7 @@ struct Dev {
     double *X, *Wt; int tabcap, K;
     long cap;                      /* points per batch */
     double *v, *uu; unsigned char *stt; long *fb; unsigned long long *nfb;
-    long nbcap; part_t *bp; unsigned *bkeep; unsigned long long *boff;
+    long nbcap; part_t *bp; unsigned *bkeep; unsigned long long *boff; unsigned char *tfb;
     sqb_acc_t *acc; unsigned long long *base;
     long dcap; sqb_pt_t *dpts; unsigned char *dskip;
     long hcap; sqb_pt_t *hpts; unsigned char *hskip, *hst; double *hv, *huu;
@@ -129,11 +127,11 @@ extern "C" int sqb_dev_tables(const double *X, const double *Wt, int K){
 static int reserve_points(long n){
     if(n <= G.cap) return 0;
     long c = 1L << 16; while(c < n) c <<= 1;
-    if(G.v){ cudaFree(G.v); cudaFree(G.uu); cudaFree(G.stt); cudaFree(G.fb); cudaFree(G.bp); cudaFree(G.bkeep); cudaFree(G.boff); }
+    if(G.v){ cudaFree(G.v); cudaFree(G.uu); cudaFree(G.stt); cudaFree(G.fb); cudaFree(G.bp); cudaFree(G.bkeep); cudaFree(G.boff); cudaFree(G.tfb); }
     CKR(cudaMalloc(&G.v, c*sizeof(double))); CKR(cudaMalloc(&G.uu, c*sizeof(double)));
     CKR(cudaMalloc(&G.stt, c)); CKR(cudaMalloc(&G.fb, c*sizeof(long)));
     long nb = (c + RTILE - 1)/RTILE;
-    CKR(cudaMalloc(&G.bp, nb*sizeof(part_t))); CKR(cudaMalloc(&G.bkeep, nb*sizeof(unsigned)));
+    CKR(cudaMalloc(&G.bp, nb*sizeof(part_t))); CKR(cudaMalloc(&G.bkeep, nb*sizeof(unsigned))); CKR(cudaMalloc(&G.tfb, nb));
     CKR(cudaMalloc(&G.boff, nb*sizeof(unsigned long long)));
     G.cap = c; G.nbcap = nb;
     return 0;
@@ -143,6 +141,15 @@ static int reserve_points(long n){
 static inline int f64_which(const sqb_graph_t *g, int fma){ return fma && g->f64_fma ? 2 : 0; }
 static inline void launch_f64(const sqb_graph_t *g, int which, const sqb_eval_t *a, int grid, size_t smem, cudaStream_t s){
     if(which == 2) g->f64_fma(a, grid, 128, smem, s); else g->f64(a, grid, 128, smem, s);
+}
+
+/* resident CTAs of a graph's kernel on the whole device; *fused: the kernel sums level tiles itself */
+static long grid_cap(const sqb_graph_t *g, int which, size_t smem, int *fused = NULL){
+    sqb_kattr_t at; memset(&at, 0, sizeof at); int per = 2;
+    const int ok = g->attr(which, 128, smem, &at);
+    if(ok && at.blocks_per_sm > 0) per = at.blocks_per_sm;
+    if(fused) *fused = ok && at.fused;
+    return (long)G.nsm*per;
 }
 
 static int grid_for(const sqb_graph_t *g, int which, long npts, size_t smem){
@@ -307,7 +314,8 @@ __device__ __forceinline__ int parent_tier(const lvl_t &a, long i){
  * then double-double across threads in a fixed tree.  Thread t of the tile takes children t, t + RT,
  * t + 2 RT, ... (each warp reads 256 contiguous bytes of v per step); the order is fixed, so a run is
  * reproducible. */
-__global__ void __launch_bounds__(RT) sqb_k_reduce(const lvl_t a, part_t *bp, unsigned *bkeep){
+__global__ void __launch_bounds__(RT) sqb_k_reduce(const lvl_t a, part_t *bp, unsigned *bkeep, const unsigned char *tfb){
+    if(tfb && !tfb[blockIdx.x]) return;      /* summed by the FP64 pass already (no fallback point in it) */
     const long t0 = blockIdx.x*(long)RTILE + threadIdx.x;
     sqdd S, b1, b2;
     double A = 0, dr = 0, uu = 0;
@@ -468,11 +476,17 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
         const sqb_pt_t *cells = L->cells + c0;
         sqb_eval_t a; memset(&a, 0, sizeof a); fill_eval(&a, &L->t);
         a.pts = cells; a.n = nc; a.esize = 1; a.stride = SQB_MAXD; a.flag_at = SQB_PFLAG; a.cells = 1; a.st = L->st;
+        /* level mode: the FP64 pass sums the tiles without fallback points (the all-dd form has no FP64
+         * pass: the reduce kernel sums every tile) */
+        int can = 0;
+        const long cap = grid_cap(g, f64_which(g, L->t.fma), 2*(2*G.K + 1)*sizeof(double), &can);
+        const bool fused = !L->t.alldd && can && nch >= 2*SQB_TILE*cap;
+        if(fused){ a.part = G.bp; a.tkeep = G.bkeep; a.tfb = G.tfb; a.pw = L->pw; a.thr = L->thr; a.last = L->last; }
         if(eval_batch(g, &a, &L->t, nch)) return -1;
         lvl_t r; r.cells = (const signed char*)cells; r.n = nch; r.D = D; r.st = L->st; r.last = L->last;
         r.abskip = L->t.abskip; r.pw = L->pw; r.thr = L->thr; r.v = G.v; r.uu = G.uu; r.stt = G.stt;
         const long nb = (nch + RTILE - 1)/RTILE;
-        sqb_k_reduce<<<(unsigned)nb, RT, 0, G.s>>>(r, G.bp, G.bkeep);
+        sqb_k_reduce<<<(unsigned)nb, RT, 0, G.s>>>(r, G.bp, G.bkeep, fused ? G.tfb : NULL);
         CKR(cudaGetLastError());
         sqb_k_finish<<<1, FT, 0, G.s>>>(G.bp, G.bkeep, nb, G.boff, G.acc, G.base);
         CKR(cudaGetLastError());
@@ -715,7 +729,7 @@ extern "C" int sqb_level_tail(const void *cells, long nchildren, int D, int st, 
     r.abskip = abskip; r.pw = pw; r.thr = thr; r.v = v; r.uu = uu; r.stt = stt;
     const long nb = (nchildren + RTILE - 1)/RTILE;
     cudaStream_t s = (cudaStream_t)stream;
-    sqb_k_reduce<<<(unsigned)nb, RT, 0, s>>>(r, (part_t*)bp, bkeep);
+    sqb_k_reduce<<<(unsigned)nb, RT, 0, s>>>(r, (part_t*)bp, bkeep, NULL);
     CKR(cudaGetLastError());
     sqb_k_finish<<<1, FT, 0, s>>>((const part_t*)bp, bkeep, nb, boff, acc, base);
     CKR(cudaGetLastError());

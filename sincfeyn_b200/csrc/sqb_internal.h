@@ -20,6 +20,13 @@ enum {
  * Coordinates are integers k (|k| <= K) of esize bytes (1: the pt_t layout of the level lists and
  * checkpoints, 2: the int16 layout of the reference's GPU plug-in), stride elements per node or
  * cell; the per-node flags byte (pt_t slot PFLAG) sits at element flag_at, or flag_at < 0. */
+/* the sums of one tile of SQB_TILE consecutive children of a level batch, double-double (hi, lo) */
+#define SQB_TILE 4096
+typedef struct {
+    double S[2], A[2], drop[2], b1[2], b2[2], u[2];
+    unsigned long long ne, nq, unres, skipped;
+} sqb_part_t;
+
 typedef struct {
     const void *pts;
     long n;                       /* nodes, or cells */
@@ -40,6 +47,14 @@ typedef struct {
     long *fb;                     /* test mode: points that need the fallback (unordered) */
     unsigned long long *nfb;
     long fbcap;
+    /* level mode (test mode over cells, part != NULL): the FP64 pass also sums every tile of SQB_TILE
+     * children that needs no fallback (part, tkeep: kept count), and flags the others (tfb = 1) for the
+     * reduce kernel, which sums them after the double-double pass */
+    sqb_part_t *part;
+    unsigned *tkeep;
+    unsigned char *tfb;
+    double pw, thr;               /* the level's weight step^D and keep threshold */
+    int last;                     /* the last level: shadow-tier sums, no kept children */
 } sqb_eval_t;
 
 /* The double-double kernel over a list of points of the same launch geometry (fb/nfb from the FP64
@@ -56,6 +71,7 @@ typedef struct {
 
 typedef struct {
     int regs, local_bytes, max_threads, blocks_per_sm;
+    int fused;                    /* FP64 kernel: sums level tiles itself (level mode available) */
 } sqb_kattr_t;
 
 typedef struct {

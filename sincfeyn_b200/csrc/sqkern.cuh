@@ -41,6 +41,10 @@
 #ifndef SQB_MINB
 #define SQB_MINB 1            /* FP64 kernel: resident blocks per SM the register allocation must allow */
 #endif
+#ifndef SQB_FUSE
+#define SQB_FUSE 1            /* FP64 kernel: level mode (tile sums in shared memory) compiled in; a kernel
+                                 that spills its registers is built without it, keeping L1 for its stack */
+#endif
 #define SQB_QEPS 4.93e-32   /* double-double epsilon of the fallback's error model (driver/common.h:8) */
 
 /* coordinates and weight of point i; returns false for a child below the box */
@@ -95,40 +99,133 @@ __device__ __forceinline__ void sqb_tables(const sqb_eval_t &a, double *sX, doub
     __syncthreads();
 }
 
+/* the tile's sums in level mode: thread t's running sums sit in shared memory (column t), out of the
+ * registers that the integrand needs; at the tile's end warp 0 adds the columns in a fixed order */
+struct sqb_tile_acc {
+    double S[2][SQB_BLOCK], A[SQB_BLOCK], dr[SQB_BLOCK], b1[2][SQB_BLOCK], b2[2][SQB_BLOCK];
+    unsigned ne[SQB_BLOCK], nsk[SQB_BLOCK], keep[SQB_BLOCK];
+    int fb;
+};
+
+__device__ __forceinline__ void sqb_acc_dd(double (*x)[SQB_BLOCK], int t, double y){
+    const sqdd z = sqdd_add_d(sqdd(x[0][t], x[1][t]), y);
+    x[0][t] = z.hi; x[1][t] = z.lo;
+}
+
+/* warp 0: the tile's sums in a fixed order (lane l adds columns l, l+32, l+64, l+96, then a shuffle
+ * tree), written to part[tile]; the block's threads have synchronised before */
+__device__ __forceinline__ void sqb_tile_flush(const sqb_eval_t &a, sqb_tile_acc &ta, long tile){
+    if(threadIdx.x >= 32) return;
+    const int l = threadIdx.x;
+    sqdd S, b1, b2; double A = 0, dr = 0; unsigned ne = 0, nsk = 0, keep = 0;
+    for(int q = l; q < SQB_BLOCK; q += 32){
+        S = S + sqdd(ta.S[0][q], ta.S[1][q]); b1 = b1 + sqdd(ta.b1[0][q], ta.b1[1][q]); b2 = b2 + sqdd(ta.b2[0][q], ta.b2[1][q]);
+        A += ta.A[q]; dr += ta.dr[q]; ne += ta.ne[q]; nsk += ta.nsk[q]; keep += ta.keep[q];
+    }
+    sqdd Ad(A), dd(dr);
+    for(int off = 16; off; off >>= 1){
+        S = S + sqdd(__shfl_down_sync(0xffffffffu, S.hi, off), __shfl_down_sync(0xffffffffu, S.lo, off));
+        Ad = Ad + sqdd(__shfl_down_sync(0xffffffffu, Ad.hi, off), __shfl_down_sync(0xffffffffu, Ad.lo, off));
+        dd = dd + sqdd(__shfl_down_sync(0xffffffffu, dd.hi, off), __shfl_down_sync(0xffffffffu, dd.lo, off));
+        b1 = b1 + sqdd(__shfl_down_sync(0xffffffffu, b1.hi, off), __shfl_down_sync(0xffffffffu, b1.lo, off));
+        b2 = b2 + sqdd(__shfl_down_sync(0xffffffffu, b2.hi, off), __shfl_down_sync(0xffffffffu, b2.lo, off));
+        ne += __shfl_down_sync(0xffffffffu, ne, off); nsk += __shfl_down_sync(0xffffffffu, nsk, off);
+        keep += __shfl_down_sync(0xffffffffu, keep, off);
+    }
+    if(l == 0){
+        sqb_part_t p;
+        p.S[0] = S.hi; p.S[1] = S.lo; p.A[0] = Ad.hi; p.A[1] = Ad.lo; p.drop[0] = dd.hi; p.drop[1] = dd.lo;
+        p.b1[0] = b1.hi; p.b1[1] = b1.lo; p.b2[0] = b2.hi; p.b2[1] = b2.lo; p.u[0] = 0; p.u[1] = 0;
+        p.ne = ne; p.nq = 0; p.unres = 0; p.skipped = nsk;
+        a.part[tile] = p; a.tkeep[tile] = keep; a.tfb[tile] = 0;
+    }
+}
+
+/* The FP64 pass.  The CTAs take tiles of consecutive points in turn (tile b, b + gridDim.x, ...): SQB_TILE
+ * points in level mode, SQB_BLOCK otherwise; in a tile, thread t evaluates points t, t + SQB_BLOCK, ...
+ * (consecutive threads, consecutive points).
+ * In level mode (a.part) each CTA also sums its tiles: the children that need no fallback add v*pw and
+ * the rest into the thread's column of shared memory; a tile with a fallback point is only flagged
+ * (a.tfb), and the reduce kernel sums it after the double-double pass. */
 template<class F, int D>
 __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const sqb_eval_t a){
     extern __shared__ double sqb_sm[];
     double *sX = sqb_sm, *sW = sqb_sm + (2*a.K + 1);
+#if SQB_FUSE
+    __shared__ sqb_tile_acc ta;
+    const bool lvl = a.part != NULL;
+#else
+    const bool lvl = false;
+#endif
     sqb_tables(a, sX, sW);
     const long n = a.cells ? (a.n << D) : a.n;
-    for(long i = blockIdx.x*(long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x*blockDim.x){
-        long c; double sf[D], w;
-        const bool in = sqb_point<D>(a, sX, sW, i, &c, sf, &w);
-        if(!in){
-            a.v[i] = 0;
-            if(a.raw) a.ab[i] = 0; else a.stt[i] = 0;
-            continue;
+    const long tl = lvl ? SQB_TILE : SQB_BLOCK;          /* other modes: one point per thread per step */
+    const long ntiles = (n + tl - 1)/tl;
+    const int t = threadIdx.x;
+    for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x){
+#if SQB_FUSE
+        if(lvl){
+            ta.S[0][t] = ta.S[1][t] = ta.A[t] = ta.dr[t] = ta.b1[0][t] = ta.b1[1][t] = ta.b2[0][t] = ta.b2[1][t] = 0;
+            ta.ne[t] = ta.nsk[t] = ta.keep[t] = 0;
+            if(t == 0) ta.fb = 0;
+            __syncthreads();
         }
-        const int sk = sqb_skip<D>(a, c);
-        const bool noab = sk && !a.abcheck;
-        double ab = 0, f;
-        if(noab) f = F::template f<double, 0>(sf, &ab);
-        else     f = F::template f<double, 1>(sf, &ab);
-        const double fw = f*w;
-        if(a.raw){ a.v[i] = fw; a.ab[i] = ab*w; continue; }
-        unsigned char s = SQB_PRESENT | (sk ? SQB_SKIPPED : 0);
-        double v;
-        if(noab) v = isfinite(fw) ? fw : 0.0;
-        else {
-            const double bnd = ab*w*16*DBL_EPSILON/a.ddslack;
-            if(!(bnd <= a.near_thr)) s |= SQB_NEAR;
-            if(!(bnd <= a.abserr)){
-                s |= SQB_FALLBACK; v = 0.0;
-                const unsigned long long q = atomicAdd(a.nfb, 1ULL);
-                if((long)q < a.fbcap) a.fb[q] = i;
-            } else v = isfinite(fw) ? fw : 0.0;
+#endif
+        for(int j = 0; j < tl/SQB_BLOCK; j++){
+            const long i = tile*tl + (long)j*SQB_BLOCK + t;
+            if(i >= n) break;
+            long c; double sf[D], w;
+            const bool in = sqb_point<D>(a, sX, sW, i, &c, sf, &w);
+            if(!in){
+                a.v[i] = 0;
+                if(a.raw) a.ab[i] = 0; else a.stt[i] = 0;
+                continue;
+            }
+            const int sk = sqb_skip<D>(a, c);
+            const bool noab = sk && !a.abcheck;
+            double ab = 0, f;
+            if(noab) f = F::template f<double, 0>(sf, &ab);
+            else     f = F::template f<double, 1>(sf, &ab);
+            const double fw = f*w;
+            if(a.raw){ a.v[i] = fw; a.ab[i] = ab*w; continue; }
+            unsigned char s = SQB_PRESENT | (sk ? SQB_SKIPPED : 0);
+            double v;
+            bool fallback = false;
+            if(noab) v = isfinite(fw) ? fw : 0.0;
+            else {
+                const double bnd = ab*w*16*DBL_EPSILON/a.ddslack;
+                if(!(bnd <= a.near_thr)) s |= SQB_NEAR;
+                if(!(bnd <= a.abserr)){
+                    s |= SQB_FALLBACK; v = 0.0; fallback = true;
+                    const unsigned long long q = atomicAdd(a.nfb, 1ULL);
+                    if((long)q < a.fbcap) a.fb[q] = i;
+                } else v = isfinite(fw) ? fw : 0.0;
+            }
+            a.v[i] = v; a.stt[i] = s;
+#if SQB_FUSE
+            if(lvl){
+                if(fallback){ ta.fb = 1; continue; }
+                const double vp = v*a.pw, av = fabs(v);
+                sqb_acc_dd(ta.S, t, vp); ta.A[t] += av; ta.ne[t]++; ta.nsk[t] += sk ? 1 : 0;
+                if(a.last){
+                    const int te = (((const signed char*)a.pts)[c*(long)a.stride + a.flag_at] >> 1) & 3;
+                    if(te >= 1) sqb_acc_dd(ta.b1, t, vp);
+                    if(te >= 2) sqb_acc_dd(ta.b2, t, vp);
+                } else if(av >= a.thr) ta.keep[t]++;
+                else ta.dr[t] += av*a.pw;
+            }
+#else
+            (void)fallback;
+#endif
         }
-        a.v[i] = v; a.stt[i] = s;
+#if SQB_FUSE
+        if(lvl){
+            __syncthreads();
+            if(ta.fb){ if(t == 0) a.tfb[tile] = 1; }
+            else sqb_tile_flush(a, ta, tile);
+            __syncthreads();
+        }
+#endif
     }
 }
 
@@ -190,7 +287,7 @@ extern "C" int SQB_##NAME##_attrfma(int block, size_t smem, sqb_kattr_t *o){    
     if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sqb_k_f64<SQG_NS(NAME)::F, D>, block, smem) \
        != cudaSuccess) return 0;                                                                   \
     o->regs = fa.numRegs; o->local_bytes = (int)fa.localSizeBytes;                                 \
-    o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; return 1; }
+    o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; o->fused = SQB_FUSE; return 1; }
 #else
 #define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
 extern "C" void SQB_##NAME##_f64fma(const sqb_eval_t *, int, int, size_t, void *) __attribute__((weak)); \
@@ -216,7 +313,7 @@ static int attr(int which, int block, size_t smem, sqb_kattr_t *o){             
               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sqb_k_f64<F, D>, block, smem);  \
     if(e != cudaSuccess) return 0;                                                                 \
     o->regs = fa.numRegs; o->local_bytes = (int)fa.localSizeBytes;                                 \
-    o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; return 1; }                     \
+    o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; o->fused = SQB_FUSE; return 1; } \
 }                                                                                                  \
 extern "C" const sqb_graph_t SQB_##NAME = {#NAME, VOLKOV, L, D, W, NP, FIX, 0,                     \
     SQG_NS(NAME)::f64, SQG_NS(NAME)::dd, SQG_NS(NAME)::attr, SQB_##NAME##_f64fma};
