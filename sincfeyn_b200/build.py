@@ -130,7 +130,7 @@ def generate(srcs):
             with open(cuh, 'w') as f:
                 f.write(text)
         with open(cuh) as f:
-            m = re.search(r'^SQ_GRAPH\((\w+), "((?:[^"\\]|\\.)*)", (\d+), (\d+),', f.read(), re.M)
+            m = re.search(r'^SQ_GRAPH(?:_SPLIT)?\((\w+), "((?:[^"\\]|\\.)*)", (\d+), (\d+),', f.read(), re.M)
         name, D = m.group(1), int(m.group(4))
         if name in seen:
             continue
@@ -189,6 +189,7 @@ def count_flops(graphs):
          '#include <stdio.h>', '#include "sqcount.h"', 'long sq_flops, sq_trans;',
          '#define SQ_TABLE static const', '#define SQ_FUNC', '#define SQ_FUNC_K', '#define SQ_CHUNK', '#define SQ_CHUNK_DD', '#define RABS(x) sq_rabs(x)',
          '#define SQ_EXP(x) sq_exp(x)', '#define SQ_LOG(x) sq_log(x)', '#define SQG_NS(n) sqg_##n',
+         '#define SQ_GRAPH_SPLIT(NAME, VOLKOV, L, D, W, NP, FIX, NPARTS) SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)',
          '#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX) \\',
          'static void count_##NAME(void){ sq_count sf[D], ab; for(int d = 0; d < D; d++) sf[d] = sq_count(0.7 + 0.37*d); \\',
          '  sq_flops = 0; sq_trans = 0; sqg_##NAME::K<sq_count, 1>::f_##NAME(sf, &ab); long a1 = sq_flops, t1 = sq_trans; \\',

@@ -166,6 +166,11 @@ def split_plan(k, max_parts=6):
     out.append('static SQ_FUNC_K REAL FN(ffin_%s)(const REAL *sf, const REAL TT_, const REAL TA_, REAL *ab){' % k.name)
     out.append(fin)
     out.append('}')
+    # pass P by a template parameter (only the selected pass is compiled into a kernel)
+    out.append('template<int P> static SQ_FUNC_K void FN(fpart_%s)(const REAL *sf, REAL *tot_, REAL *tota_){' % k.name)
+    for P in range(len(groups)):
+        out.append('  %sif constexpr(P == %d) FN(fpart%d_%s)(sf, tot_, tota_);' % ('else ' if P else '', P, P, k.name))
+    out.append('}')
     return groups, '\n'.join(out)
 
 
@@ -190,17 +195,20 @@ def emit(src):
         out += ['/* the same point function in %d passes over groups of its nodes (kgen.split_plan) */' % len(plan[0]),
                 plan[1]]
     out += ['};']
-    if plan:
-        out.append('#define SQ_SPLIT_%s %d' % (k.name, len(plan[0])))
+
     if any(k.chunk(f) for _, f in k.funcs):
         out += ['template<class SqReal_, int SQ_AB> struct KD {',
                 k.body('SQ_CHUNK_DD').strip('\n'),
                 '};']
     else:
         out += ['template<class SqReal_, int SQ_AB> using KD = K<SqReal_, SQ_AB>;']
-    out += ['#undef REAL', '#undef FN', '}',
-            'SQ_GRAPH(%s, "%s", %d, %d, %d, %d, %d)' % (k.name, k.volkov.replace('"', '\\"'),
-                                                        k.L, k.D, k.weight, k.n, k.fixed)]
+    out += ['#undef REAL', '#undef FN', '}']
+    if plan:
+        out.append('SQ_GRAPH_SPLIT(%s, "%s", %d, %d, %d, %d, %d, %d)' % (k.name, k.volkov.replace('"', '\\"'),
+                                                                    k.L, k.D, k.weight, k.n, k.fixed, len(plan[0])))
+    else:
+        out.append('SQ_GRAPH(%s, "%s", %d, %d, %d, %d, %d)' % (k.name, k.volkov.replace('"', '\\"'),
+                                                            k.L, k.D, k.weight, k.n, k.fixed))
     return k, '\n'.join(out) + '\n'
 
 

@@ -48,7 +48,7 @@ extern "C" void sqb_default_opts(sqb_opts_t *o){
     o->abserr0 = 1e-15; o->abrel = 1e-3; o->nearf = 1e-3; o->ddslack = 1;
     o->abskip = 1; o->abcheck = 0; o->dropunres = 1; o->growskip = 2;
     o->alldd = 0; o->device = 0; o->max_children = 0; o->verbose = 0;
-    o->fma = 1;
+    o->fma = 1; o->split = 1;
 }
 
 extern "C" int sqb_graph_count(void){ return sqb_ngraphs(); }
@@ -78,7 +78,7 @@ struct Run {
 static void set_test(Run &R, double abserr){
     R.t.abserr = abserr; R.t.nearf = R.o.nearf; R.t.ddslack = R.o.ddslack;
     R.t.abskip = R.o.abskip; R.t.abcheck = R.o.abcheck; R.t.dropunres = R.o.dropunres; R.t.alldd = R.o.alldd;
-    R.t.fma = R.o.fma;
+    R.t.fma = R.o.fma; R.t.split = R.o.split;
 }
 
 static int eval(Run &R, const std::vector<sqb_pt_t> &p, const unsigned char *skip, std::vector<double> &v, std::vector<unsigned char> &nr){

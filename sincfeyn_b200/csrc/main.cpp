@@ -68,6 +68,7 @@ int main(int argc, char **argv){
     if((e = getenv("SQB_DEVICE"))) o.device = atoi(e);
     if((e = getenv("SQB_VERBOSE"))) o.verbose = atoi(e);
     if((e = getenv("SQB_FMA"))) o.fma = atoi(e);
+    if((e = getenv("SQB_SPLIT"))) o.split = atoi(e);
     /* checkpoints at every level end, on by default as in the reference (driver/main.c:28,184) */
     o.ckpt_every = 600;
     if((e = getenv("SINCQED_CKPT"))) o.ckpt_every = atof(e);

@@ -77,6 +77,7 @@ struct Dev {
     long cap;                      /* points per batch */
     double *v, *uu; unsigned char *stt; long *fb; unsigned long long *nfb;
     long nbcap; part_t *bp; unsigned *bkeep; unsigned long long *boff; unsigned char *tfb;
+    long ttcap; double *tt, *ta;   /* split FP64 pass: running sums per point */
     sqb_acc_t *acc; unsigned long long *base;
     long dcap; sqb_pt_t *dpts; unsigned char *dskip;
     long hcap; sqb_pt_t *hpts; unsigned char *hskip, *hst; double *hv, *huu;
@@ -167,6 +168,11 @@ static void fill_eval(sqb_eval_t *a, const sqb_test_t *t){
     a->v = G.v; a->ab = NULL; a->stt = G.stt; a->fb = G.fb; a->nfb = G.nfb; a->fbcap = G.cap;
 }
 
+/* whether a batch's FP64 pass runs in passes (the graph has them, they are asked for, a level batch) */
+static inline bool use_split(const sqb_graph_t *g, const sqb_eval_t *a, const sqb_test_t *t){
+    return t->split && g->nparts > 0 && a->cells && !t->alldd;
+}
+
 /* FP64 pass (or the all-dd pass) and the fallback pass for one batch already described by a */
 static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, long npts){
     size_t smem = 2*(2*G.K + 1)*sizeof(double);
@@ -181,9 +187,26 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
     }
     CKR(cudaMemsetAsync(G.nfb, 0, sizeof(unsigned long long), G.s));
     if(KTIME) CKR(cudaEventRecord(G.k0, G.s));
-    const int w = f64_which(g, t->fma);
-    launch_f64(g, w, a, grid_for(g, w, npts, smem), smem, G.s);
-    CKR(cudaGetLastError());
+    if(use_split(g, a, t)){
+        if(npts > G.ttcap){
+            if(G.tt){ cudaFree(G.tt); cudaFree(G.ta); }
+            long c = 1L << 16; while(c < npts) c <<= 1;
+            CKR(cudaMalloc(&G.tt, c*sizeof(double))); CKR(cudaMalloc(&G.ta, c*sizeof(double)));
+            G.ttcap = c;
+        }
+        for(int P = 0; P <= g->nparts; P++){
+            sqb_kattr_t at; memset(&at, 0, sizeof at); int per = 2;
+            if(g->split_attr(P, t->fma, 128, smem, &at) && at.blocks_per_sm > 0) per = at.blocks_per_sm;
+            long want = (npts + 127)/128, full = (long)G.nsm*per;
+            g->split(P, t->fma, a, G.tt, G.ta, (int)(want < full ? want : full), 128, smem, G.s);
+            CKR(cudaGetLastError());
+        }
+        G.launches += g->nparts;
+    } else {
+        const int w = f64_which(g, t->fma);
+        launch_f64(g, w, a, grid_for(g, w, npts, smem), smem, G.s);
+        CKR(cudaGetLastError());
+    }
     if(KTIME) CKR(cudaEventRecord(G.k1, G.s));
     d.list = G.fb; d.nlist = G.nfb; d.listcap = G.cap; d.all = 0;
     /* the queue length is known only on the device: a persistent grid reads it */
@@ -288,6 +311,8 @@ extern "C" int sqb_preload(const char *graph){
         if(graph && strcmp(graph, g->name)) continue;
         sqb_kattr_t at;
         for(int which = 0; which < 3; which++) if(g->attr(which, 128, 4096, &at)) n++;
+        for(int P = 0; P <= g->nparts && g->nparts > 0; P++)
+            for(int fma = 0; fma < 2; fma++) if(g->split_attr(P, fma, 128, 4096, &at)) n++;
     }
     return n;
 }
@@ -480,7 +505,7 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
          * pass: the reduce kernel sums every tile) */
         int can = 0;
         const long cap = grid_cap(g, f64_which(g, L->t.fma), 2*(2*G.K + 1)*sizeof(double), &can);
-        const bool fused = !L->t.alldd && can && nch >= 2*SQB_TILE*cap;
+        const bool fused = !L->t.alldd && can && !use_split(g, &a, &L->t) && nch >= 2*SQB_TILE*cap;
         if(fused){ a.part = G.bp; a.tkeep = G.bkeep; a.tfb = G.tfb; a.pw = L->pw; a.thr = L->thr; a.last = L->last; }
         if(eval_batch(g, &a, &L->t, nch)) return -1;
         lvl_t r; r.cells = (const signed char*)cells; r.n = nch; r.D = D; r.st = L->st; r.last = L->last;

@@ -86,6 +86,13 @@ typedef struct {
     /* the FP64 kernel compiled with contraction (-fmad=true: fused multiply-adds), from the graph's second
      * translation unit; NULL if the library was built without it */
     void (*f64_fma)(const sqb_eval_t *a, int grid, int block, size_t smem, void *stream);
+    /* nparts > 0: the FP64 pass of a level batch may run as nparts passes (P = 0 .. nparts-1), each adding
+     * a group of the point function's nodes to the point's running sums tt[i], ta[i], and a final pass
+     * (P = nparts) with the tests; fma: the contracted build */
+    int nparts;
+    void (*split)(int P, int fma, const sqb_eval_t *a, double *tt, double *ta, int grid, int block, size_t smem,
+                  void *stream);
+    int (*split_attr)(int P, int fma, int block, size_t smem, sqb_kattr_t *out);
 } sqb_graph_t;
 
 #ifdef __cplusplus

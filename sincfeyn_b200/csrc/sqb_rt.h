@@ -17,6 +17,7 @@ typedef struct {
     int abskip, abcheck, dropunres;
     int alldd;                        /* every point in double-double (the plain all-dd form) */
     int fma;                          /* FP64 pass: the contracted kernel (fused multiply-adds) when present */
+    int split;                        /* FP64 pass of a level batch in passes, for graphs that have them */
 } sqb_test_t;
 
 /* level accumulators, double-double (hi, lo) pairs */

@@ -99,6 +99,29 @@ __device__ __forceinline__ void sqb_tables(const sqb_eval_t &a, double *sX, doub
     __syncthreads();
 }
 
+/* the per-point tests of finish() (driver/eval.c:33-53) on the FP64 value fw = f w and |.| sum abw = ab w
+ * of point i: skipped points keep fw; otherwise the bound abw 16 eps / DDSLACK sets the near flag and,
+ * above ABSERR, queues the point for the double-double pass (value 0 until then).  Writes v[i] and
+ * stt[i]; returns the value */
+__device__ __forceinline__ double sqb_point_test(const sqb_eval_t &a, long i, int sk, bool noab, double fw, double abw,
+                                                 bool *fallback){
+    unsigned char s = SQB_PRESENT | (sk ? SQB_SKIPPED : 0);
+    double v;
+    *fallback = false;
+    if(noab) v = isfinite(fw) ? fw : 0.0;
+    else {
+        const double bnd = abw*16*DBL_EPSILON/a.ddslack;
+        if(!(bnd <= a.near_thr)) s |= SQB_NEAR;
+        if(!(bnd <= a.abserr)){
+            s |= SQB_FALLBACK; v = 0.0; *fallback = true;
+            const unsigned long long q = atomicAdd(a.nfb, 1ULL);
+            if((long)q < a.fbcap) a.fb[q] = i;
+        } else v = isfinite(fw) ? fw : 0.0;
+    }
+    a.v[i] = v; a.stt[i] = s;
+    return v;
+}
+
 /* the tile's sums in level mode: thread t's running sums sit in shared memory (column t), out of the
  * registers that the integrand needs; at the tile's end warp 0 adds the columns in a fixed order */
 struct sqb_tile_acc {
@@ -188,20 +211,8 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const sqb_eval_
             else     f = F::template f<double, 1>(sf, &ab);
             const double fw = f*w;
             if(a.raw){ a.v[i] = fw; a.ab[i] = ab*w; continue; }
-            unsigned char s = SQB_PRESENT | (sk ? SQB_SKIPPED : 0);
-            double v;
-            bool fallback = false;
-            if(noab) v = isfinite(fw) ? fw : 0.0;
-            else {
-                const double bnd = ab*w*16*DBL_EPSILON/a.ddslack;
-                if(!(bnd <= a.near_thr)) s |= SQB_NEAR;
-                if(!(bnd <= a.abserr)){
-                    s |= SQB_FALLBACK; v = 0.0; fallback = true;
-                    const unsigned long long q = atomicAdd(a.nfb, 1ULL);
-                    if((long)q < a.fbcap) a.fb[q] = i;
-                } else v = isfinite(fw) ? fw : 0.0;
-            }
-            a.v[i] = v; a.stt[i] = s;
+            bool fallback;
+            const double v = sqb_point_test(a, i, sk, noab, fw, ab*w, &fallback);
 #if SQB_FUSE
             if(lvl){
                 if(fallback){ ta.fb = 1; continue; }
@@ -263,6 +274,72 @@ __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_dd(const sqb_dd_t a){
     }
 }
 
+/* A graph whose point function is a flat sum of independent forest nodes (kgen.split_plan: g3_lbl) can
+ * run the FP64 pass of a level batch as NP passes and a final one.  Pass P evaluates the nodes of group P
+ * at every point and adds their contributions to the point's running (tot, tota) in tt[i], ta[i]; the
+ * final pass applies f_'s own arithmetic to them and the tests of finish().  The operations and their
+ * order are those of the single function, so the values are the same; each pass's code is a fraction of
+ * the whole, which fits the instruction caches (the single kernel of g3_lbl waits on instruction fetch). */
+template<class F, int D, int P>
+__global__ void __launch_bounds__(SQB_BLOCK) sqb_k_part(const sqb_eval_t a, double *tt, double *ta){
+    extern __shared__ double sqb_sm[];
+    double *sX = sqb_sm, *sW = sqb_sm + (2*a.K + 1);
+    sqb_tables(a, sX, sW);
+    const long n = a.cells ? (a.n << D) : a.n;
+    for(long i = blockIdx.x*(long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x*blockDim.x){
+        long c; double sf[D], w;
+        if(!sqb_point<D>(a, sX, sW, i, &c, sf, &w)) continue;
+        const int sk = sqb_skip<D>(a, c);
+        double T = P ? tt[i] : 0.0, A = P ? ta[i] : 0.0;
+        if(sk && !a.abcheck) F::template part<P, 0>(sf, &T, &A);
+        else                 F::template part<P, 1>(sf, &T, &A);
+        tt[i] = T; ta[i] = A;
+    }
+}
+
+template<class F, int D>
+__global__ void __launch_bounds__(SQB_BLOCK) sqb_k_fin(const sqb_eval_t a, const double *tt, const double *ta){
+    extern __shared__ double sqb_sm[];
+    double *sX = sqb_sm, *sW = sqb_sm + (2*a.K + 1);
+    sqb_tables(a, sX, sW);
+    const long n = a.cells ? (a.n << D) : a.n;
+    for(long i = blockIdx.x*(long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x*blockDim.x){
+        long c; double sf[D], w;
+        if(!sqb_point<D>(a, sX, sW, i, &c, sf, &w)){ a.v[i] = 0; a.stt[i] = 0; continue; }
+        const int sk = sqb_skip<D>(a, c);
+        const bool noab = sk && !a.abcheck;
+        double ab = 0, f;
+        if(noab) f = F::template fin<0>(sf, tt[i], ta[i], &ab);
+        else     f = F::template fin<1>(sf, tt[i], ta[i], &ab);
+        bool fallback;
+        sqb_point_test(a, i, sk, noab, f*w, ab*w, &fallback);
+    }
+}
+
+/* launch pass P (P < NP) or the final pass (P == NP) */
+template<class F, int D, int NP>
+static void sqb_split_launch(int P, const sqb_eval_t *a, double *tt, double *ta, int grid, int block, size_t smem, cudaStream_t st){
+#define SQB_PASS_(Q) if constexpr((Q) < NP) if(P == (Q)){ sqb_k_part<F, D, (Q) < NP ? (Q) : 0><<<grid, block, smem, st>>>(*a, tt, ta); return; }
+    SQB_PASS_(0) SQB_PASS_(1) SQB_PASS_(2) SQB_PASS_(3) SQB_PASS_(4) SQB_PASS_(5) SQB_PASS_(6) SQB_PASS_(7)
+#undef SQB_PASS_
+    sqb_k_fin<F, D><<<grid, block, smem, st>>>(*a, tt, ta);
+}
+template<class K_>
+static int sqb_attr_of(K_ kernel, int block, size_t smem, sqb_kattr_t *o){
+    cudaFuncAttributes fa; int nb = 0;
+    if(cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return 0;
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, smem) != cudaSuccess) return 0;
+    o->regs = fa.numRegs; o->local_bytes = (int)fa.localSizeBytes; o->max_threads = fa.maxThreadsPerBlock;
+    o->blocks_per_sm = nb; o->fused = 0; return 1;
+}
+template<class F, int D, int NP>
+static int sqb_split_attr(int P, int block, size_t smem, sqb_kattr_t *o){
+#define SQB_PASS_(Q) if constexpr((Q) < NP) if(P == (Q)) return sqb_attr_of(sqb_k_part<F, D, (Q) < NP ? (Q) : 0>, block, smem, o);
+    SQB_PASS_(0) SQB_PASS_(1) SQB_PASS_(2) SQB_PASS_(3) SQB_PASS_(4) SQB_PASS_(5) SQB_PASS_(6) SQB_PASS_(7)
+#undef SQB_PASS_
+    return sqb_attr_of(sqb_k_fin<F, D>, block, smem, o);
+}
+
 /* SQ_GRAPH(name, volkov, L, D, weight, n, fixed): the generated file ends with it, after namespace
  * SQG_NS(name) with the class template K<Real, SQ_AB> holding f_<name>.
  *
@@ -271,6 +348,16 @@ __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_dd(const sqb_dd_t a){
  * The second (SQB_FMA_TU, compiled with -fmad=true, namespace sqgf_<name> so that no symbol is shared)
  * holds only the FP64 kernel with multiplies and adds contracted into fused multiply-adds, exported as
  * SQB_<name>_f64fma and SQB_<name>_attrfma; the registry entry refers to them weakly. */
+/* the split form's point functions (SQ_GRAPH_SPLIT): pass P and the final pass in FP64 */
+#define SQ_SPLIT_F(NAME)                                                                           \
+namespace SQG_NS(NAME) {                                                                           \
+struct FS {                                                                                        \
+    template<int P, int AB> static __device__ __forceinline__ void part(const double *sf, double *T, double *A){ \
+        K<double, AB>::template fpart_##NAME<P>(sf, T, A); }                                       \
+    template<int AB> static __device__ __forceinline__ double fin(const double *sf, double T, double A, double *ab){ \
+        return K<double, AB>::ffin_##NAME(sf, T, A, ab); }                                         \
+};                                                                                                 \
+}
 #if defined(SQB_FMA_TU)
 #define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
 namespace SQG_NS(NAME) {                                                                           \
@@ -288,8 +375,16 @@ extern "C" int SQB_##NAME##_attrfma(int block, size_t smem, sqb_kattr_t *o){    
        != cudaSuccess) return 0;                                                                   \
     o->regs = fa.numRegs; o->local_bytes = (int)fa.localSizeBytes;                                 \
     o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; o->fused = SQB_FUSE; return 1; }
+#define SQ_GRAPH_SPLIT(NAME, VOLKOV, L, D, W, NP, FIX, NPARTS)                                      \
+SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                           \
+SQ_SPLIT_F(NAME)                                                                                   \
+extern "C" void SQB_##NAME##_splitfma(int P, const sqb_eval_t *a, double *tt, double *ta, int grid, int block, \
+                                      size_t smem, void *st){                                      \
+    sqb_split_launch<SQG_NS(NAME)::FS, D, NPARTS>(P, a, tt, ta, grid, block, smem, (cudaStream_t)st); } \
+extern "C" int SQB_##NAME##_splitattrfma(int P, int block, size_t smem, sqb_kattr_t *o){          \
+    return sqb_split_attr<SQG_NS(NAME)::FS, D, NPARTS>(P, block, smem, o); }
 #else
-#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
+#define SQ_GRAPH_CORE(NAME, D)                                                                      \
 extern "C" void SQB_##NAME##_f64fma(const sqb_eval_t *, int, int, size_t, void *) __attribute__((weak)); \
 extern "C" int SQB_##NAME##_attrfma(int, size_t, sqb_kattr_t *) __attribute__((weak));             \
 namespace SQG_NS(NAME) {                                                                           \
@@ -314,7 +409,27 @@ static int attr(int which, int block, size_t smem, sqb_kattr_t *o){             
     if(e != cudaSuccess) return 0;                                                                 \
     o->regs = fa.numRegs; o->local_bytes = (int)fa.localSizeBytes;                                 \
     o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; o->fused = SQB_FUSE; return 1; } \
+}
+#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
+SQ_GRAPH_CORE(NAME, D)                                                                             \
+extern "C" const sqb_graph_t SQB_##NAME = {#NAME, VOLKOV, L, D, W, NP, FIX, 0,                     \
+    SQG_NS(NAME)::f64, SQG_NS(NAME)::dd, SQG_NS(NAME)::attr, SQB_##NAME##_f64fma, 0, NULL, NULL};
+#define SQ_GRAPH_SPLIT(NAME, VOLKOV, L, D, W, NP, FIX, NPARTS)                                      \
+SQ_GRAPH_CORE(NAME, D)                                                                             \
+SQ_SPLIT_F(NAME)                                                                                   \
+extern "C" void SQB_##NAME##_splitfma(int, const sqb_eval_t *, double *, double *, int, int, size_t, void *) \
+    __attribute__((weak));                                                                         \
+extern "C" int SQB_##NAME##_splitattrfma(int, int, size_t, sqb_kattr_t *) __attribute__((weak));   \
+namespace SQG_NS(NAME) {                                                                           \
+static void split(int P, int fma, const sqb_eval_t *a, double *tt, double *ta, int grid, int block, size_t smem, \
+                  void *st){                                                                       \
+    if(fma && SQB_##NAME##_splitfma) SQB_##NAME##_splitfma(P, a, tt, ta, grid, block, smem, st);    \
+    else sqb_split_launch<FS, D, NPARTS>(P, a, tt, ta, grid, block, smem, (cudaStream_t)st); }     \
+static int split_attr(int P, int fma, int block, size_t smem, sqb_kattr_t *o){                     \
+    if(fma && SQB_##NAME##_splitattrfma) return SQB_##NAME##_splitattrfma(P, block, smem, o);       \
+    return sqb_split_attr<FS, D, NPARTS>(P, block, smem, o); }                                      \
 }                                                                                                  \
 extern "C" const sqb_graph_t SQB_##NAME = {#NAME, VOLKOV, L, D, W, NP, FIX, 0,                     \
-    SQG_NS(NAME)::f64, SQG_NS(NAME)::dd, SQG_NS(NAME)::attr, SQB_##NAME##_f64fma};
+    SQG_NS(NAME)::f64, SQG_NS(NAME)::dd, SQG_NS(NAME)::attr, SQB_##NAME##_f64fma, NPARTS,           \
+    SQG_NS(NAME)::split, SQG_NS(NAME)::split_attr};
 #endif

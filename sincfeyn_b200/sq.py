@@ -23,7 +23,8 @@ class Opts(C.Structure):
     _fields_ = [('abserr0', C.c_double), ('abrel', C.c_double), ('nearf', C.c_double), ('ddslack', C.c_double),
                 ('abskip', C.c_int), ('abcheck', C.c_int), ('dropunres', C.c_int), ('growskip', C.c_int),
                 ('alldd', C.c_int), ('device', C.c_int), ('max_children', C.c_long), ('verbose', C.c_int),
-                ('ckpt_every', C.c_double), ('ckpt_dir', C.c_char_p), ('ckpt_stop', C.c_int), ('fma', C.c_int)]
+                ('ckpt_every', C.c_double), ('ckpt_dir', C.c_char_p), ('ckpt_stop', C.c_int), ('fma', C.c_int),
+                ('split', C.c_int)]
 
 
 class Result(C.Structure):

@@ -25,7 +25,7 @@ ABSERR, NEARF, DDSLACK = 1e-15, 1e-3, 1.0
 class PointTestParams(C.Structure):
     _fields_ = [('abserr', C.c_double), ('nearf', C.c_double), ('ddslack', C.c_double),
                 ('abskip', C.c_int), ('abcheck', C.c_int), ('dropunres', C.c_int), ('alldd', C.c_int),
-                ('fma', C.c_int)]
+                ('fma', C.c_int), ('split', C.c_int)]
 
 
 class Level(C.Structure):
@@ -60,7 +60,7 @@ def existing_level(L, cells_dev, n, next_dev, cap, last, thr):
     assert L.sqb_dev_tables(X, W, K) == 0
     L.sqb_find_graph.restype = C.c_void_p
     lv = Level(g=L.sqb_find_graph(GRAPH.encode()), cells=cells_dev, ncell=n, next=next_dev, next_cap=cap, st=ST,
-               last=last, pw=float(ST**5), thr=thr, t=PointTestParams(ABSERR, NEARF, DDSLACK, 1, 0, 1, 0, 0), max_children=0)
+               last=last, pw=float(ST**5), thr=thr, t=PointTestParams(ABSERR, NEARF, DDSLACK, 1, 0, 1, 0, 0, 0), max_children=0)
     acc, nn, ms = Acc(), C.c_long(), C.c_double()
     assert L.sqb_dev_level(C.byref(lv), C.byref(acc), C.byref(nn), C.byref(ms)) == 0
     sums = [x for f in ('S', 'A', 'drop', 'b1', 'b2', 'u') for x in getattr(acc, f)]
