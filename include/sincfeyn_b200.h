@@ -73,9 +73,10 @@ typedef struct {
                               and adds fused, as the reference's own CPU build compiles its double half);
                               0 = the kernel that rounds every operation as written, bit for bit the reference's
                               double half built with -ffp-contract=off */
-    int split;             /* SQB_SPLIT: 1 (default) = a graph whose point function is a flat sum of independent
-                              forest nodes (g3_lbl) runs the FP64 pass of its level batches as passes over groups
-                              of nodes (the same operations in the same order: the same values); 0 = one pass */
+    int split;             /* SQB_SPLIT: 1 = a graph whose point function is a flat sum of independent forest
+                              nodes (g3_lbl) runs the FP64 pass of its level batches as passes over groups of
+                              nodes (the same operations in the same order: the same values); 0 (default) = one
+                              pass, measured faster on the B200 */
 } sqb_opts_t;
 #define SQB_CKPT_STOPPED 2 /* sqb_hsum's return code under ckpt_stop */
 

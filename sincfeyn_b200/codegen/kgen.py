@@ -81,6 +81,7 @@ _PT_DEF = re.compile(r'^static REAL FN\((pt_\w+)\)\(const REAL \*x, const REAL V
 
 
 def split_plan(k, max_parts=6):
+    max_parts = min(max_parts, 8)          # sqkern.cuh launches at most eight passes
     """A point function that is a flat sum of independent forest nodes can be evaluated in passes.
 
     Returns None, or (groups, text) for the graph's FP64 split: the QREAL half's pt_<g> holds a header

@@ -48,7 +48,7 @@ extern "C" void sqb_default_opts(sqb_opts_t *o){
     o->abserr0 = 1e-15; o->abrel = 1e-3; o->nearf = 1e-3; o->ddslack = 1;
     o->abskip = 1; o->abcheck = 0; o->dropunres = 1; o->growskip = 2;
     o->alldd = 0; o->device = 0; o->max_children = 0; o->verbose = 0;
-    o->fma = 1; o->split = 1;
+    o->fma = 1; o->split = 0;
 }
 
 extern "C" int sqb_graph_count(void){ return sqb_ngraphs(); }

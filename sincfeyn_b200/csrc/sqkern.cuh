@@ -319,6 +319,7 @@ __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_fin(const sqb_eval_t a, const
 /* launch pass P (P < NP) or the final pass (P == NP) */
 template<class F, int D, int NP>
 static void sqb_split_launch(int P, const sqb_eval_t *a, double *tt, double *ta, int grid, int block, size_t smem, cudaStream_t st){
+    static_assert(NP >= 1 && NP <= 8, "at most eight passes have launchers");
 #define SQB_PASS_(Q) if constexpr((Q) < NP) if(P == (Q)){ sqb_k_part<F, D, (Q) < NP ? (Q) : 0><<<grid, block, smem, st>>>(*a, tt, ta); return; }
     SQB_PASS_(0) SQB_PASS_(1) SQB_PASS_(2) SQB_PASS_(3) SQB_PASS_(4) SQB_PASS_(5) SQB_PASS_(6) SQB_PASS_(7)
 #undef SQB_PASS_
@@ -334,6 +335,7 @@ static int sqb_attr_of(K_ kernel, int block, size_t smem, sqb_kattr_t *o){
 }
 template<class F, int D, int NP>
 static int sqb_split_attr(int P, int block, size_t smem, sqb_kattr_t *o){
+    static_assert(NP >= 1 && NP <= 8, "at most eight passes have launchers");
 #define SQB_PASS_(Q) if constexpr((Q) < NP) if(P == (Q)) return sqb_attr_of(sqb_k_part<F, D, (Q) < NP ? (Q) : 0>, block, smem, o);
     SQB_PASS_(0) SQB_PASS_(1) SQB_PASS_(2) SQB_PASS_(3) SQB_PASS_(4) SQB_PASS_(5) SQB_PASS_(6) SQB_PASS_(7)
 #undef SQB_PASS_
