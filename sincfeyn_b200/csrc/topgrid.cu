@@ -380,8 +380,9 @@ __global__ void k_tier_seed(geom_t g, const unsigned long long *key, const unsig
 }
 __global__ void k_tier_step(geom_t g, const sqb_pt_t *keep, const unsigned long long *key, const unsigned *word,
                             unsigned long long mask, const double *kv, double lim, int t, unsigned *tr,
-                            const long *cu, long nc, long *nw, unsigned long long *nnw){
+                            const long *cu, const unsigned long long *ncu, long *nw, unsigned long long *nnw){
     const int D2 = 2*g.D;
+    const long nc = (long)*ncu;          /* the frontier's size, written by the step (or seed) before */
     for(long x = blockIdx.x*(long)blockDim.x + threadIdx.x; x < nc*D2; x += (long)gridDim.x*blockDim.x){
         const long i = cu[x/D2]; const int c = (int)(x % D2), d = c >> 1, sg = (c & 1) ? 1 : -1;
         const int kk = keep[i].k[d] + g.st*sg;
@@ -415,17 +416,25 @@ extern "C" int sqb_grow_finish(double thr, int tiers, long *m_out){
     TCK(DMALLOC(&cnt, 2*sizeof(unsigned long long)));
     TCK(cudaMemsetAsync(key, 0, cap*sizeof(unsigned long long), TS)); TCK(cudaMemsetAsync(tr, 0, m*sizeof(unsigned), TS));
     k_index<<<1184, 256, 0, TS>>>(GR.g, GR.keep, m, key, word, (unsigned long long)(cap - 1), GR.err); TL++;
+    /* breadth-first steps read the frontier's size on the device, so the host checks for the end only
+     * every TSTEPS steps (steps after the end find an empty frontier and do nothing) */
+    const int TSTEPS = 8;
     for(int t = 1; t <= 2; t++){
         const double lim = (t == 1 ? 10 : 100)*thr;
-        k_tier_seed<<<1, 1, 0, TS>>>(GR.g, key, word, (unsigned long long)(cap - 1), GR.kv, lim, t, tr, cu, cnt); TL++;
-        unsigned long long nc = 0;
-        TCK(cudaMemcpyAsync(&nc, cnt, sizeof nc, cudaMemcpyDeviceToHost, TS)); TCK(cudaStreamSynchronize(TS));
-        while(nc){
-            TCK(cudaMemsetAsync(cnt + 1, 0, sizeof(unsigned long long), TS));
-            k_tier_step<<<1184, 256, 0, TS>>>(GR.g, GR.keep, key, word, (unsigned long long)(cap - 1), GR.kv, lim, t, tr, cu, (long)nc, nw, cnt + 1); TL++;
-            TCK(cudaGetLastError());
-            TCK(cudaMemcpyAsync(&nc, cnt + 1, sizeof nc, cudaMemcpyDeviceToHost, TS)); TCK(cudaStreamSynchronize(TS));
-            long *x = cu; cu = nw; nw = x;
+        unsigned long long *ca = cnt, *cb = cnt + 1;
+        k_tier_seed<<<1, 1, 0, TS>>>(GR.g, key, word, (unsigned long long)(cap - 1), GR.kv, lim, t, tr, cu, ca); TL++;
+        for(;;){
+            for(int s = 0; s < TSTEPS; s++){
+                TCK(cudaMemsetAsync(cb, 0, sizeof(unsigned long long), TS));
+                k_tier_step<<<1184, 256, 0, TS>>>(GR.g, GR.keep, key, word, (unsigned long long)(cap - 1), GR.kv, lim, t, tr,
+                                                  cu, ca, nw, cb); TL++;
+                TCK(cudaGetLastError());
+                long *x = cu; cu = nw; nw = x;
+                unsigned long long *y = ca; ca = cb; cb = y;
+            }
+            unsigned long long nc = 0;
+            TCK(cudaMemcpyAsync(&nc, ca, sizeof nc, cudaMemcpyDeviceToHost, TS)); TCK(cudaStreamSynchronize(TS));
+            if(!nc) break;
         }
     }
     k_tier_apply<<<1184, 256, 0, TS>>>(GR.keep, tr, m); TL++;
