@@ -28,6 +28,9 @@ JSON line (rank 0):
              bounded sample of the same workload
   vs_alldd   a sample of the set (or the whole set, --alldd-full) in the contracted, the as-written and the
              plain all-double-double forms, one integral at a time: time ratio
+  fold       the same batch with the symmetry fold (sym='auto': each integrand's group of axis
+             permutations, as the reference CPU build finds it): time-to-sum, evaluated points, the largest
+             relative difference from the unfolded values, the group orders
 `--impl reference` times the reference CPU build on the same metric (rank 0 only).
 
 Other measurements (one GPU, each prints its own JSON lines; not the headline):
@@ -36,7 +39,7 @@ Other measurements (one GPU, each prints its own JSON lines; not the headline):
   --workload synth   the synthetic Sinc-sum microbenchmark (d = 5, 8, 11; h = 1.0, 0.7) and its
                      precision table (FP64 only, FP64 + dd, all-dd, the reference's hsum)
   --workload vp4     the four-loop lepton-loop set (kernels/v4, kernels/w4) at h = 1.0 and 0.9, with the
-                     exactly known set values
+                     exactly known set values (--fold: with the symmetry fold)
   --workload single  one integral (--graph) warm, then timed once: a small command for profilers
   --workload points  one launch of a graph's evaluation kernel on --npoints seeded nodes (--prec)
 """
@@ -243,7 +246,7 @@ def run_vp4(args, sq, L):
         if args.vp4_h and h not in args.vp4_h:
             continue
         jobs = [(g, h, N, EPS, -1, (2.0/h)**info[g]['D']) for g in names]
-        res, ms = sq.hsum_batch(jobs, workers=workers)
+        res, ms = sq.hsum_batch(jobs, workers=workers, **({'sym': 'auto'} if args.fold else {}))
         nev = sum(r['nev'] for r in res)
         val = {g: r['S'][0]*info[g]['weight'] for g, r in zip(names, res)}
         sets = []
@@ -252,7 +255,8 @@ def run_vp4(args, sq, L):
             s = sum(val[g] for g in mem)
             sets.append({'set': label, 'graphs': len(mem), 'sum': s, 'exact': exact, 'diff': s - exact})
         slow = sorted(zip(names, res), key=lambda x: -x[1]['t'])[:5]
-        row = {'h': h, 'N': N, 'integrals': len(jobs), 'workers': workers, 'device_s': ms*1e-3, 'points': nev,
+        row = {'h': h, 'N': N, 'integrals': len(jobs), 'workers': workers, 'fold': bool(args.fold),
+               'device_s': ms*1e-3, 'points': nev,
                'points_s': nev/(ms*1e-3), 'fallback': sum(r['nq'] for r in res), 'sets': sets,
                'slowest': [[g, round(r['t'], 2), r['nev']] for g, r in slow],
                'values': {g: val[g] for g in names}}
@@ -358,6 +362,8 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-alldd', action='store_true', help='skip the all-double-double comparison')
     ap.add_argument('--alldd-full', action='store_true', help='all-double-double comparison on the whole set (~2 min)')
+    ap.add_argument('--no-fold', action='store_true', help='skip the batch with the symmetry fold')
+    ap.add_argument('--fold', action='store_true', help='--workload vp4: with the symmetry fold (sym=auto)')
     ap.add_argument('--workers', type=int, default=0, help='batch workers for --workload vp4 (default 6)')
     ap.add_argument('--vp4-h', type=float, action='append', help='--workload vp4: only these h (repeatable)')
     ap.add_argument('--graph', default='g3_00', help='--workload single/points: the graph')
@@ -461,13 +467,24 @@ def main():
         same = same and (r['S'][0] == bvals[g] or (r['S'][0] != r['S'][0] and bvals[g] != bvals[g]))
         results.append([g, r['S'][0]*weight[g], r['nev'], r['nq'], round(ms, 2), round(1e3*r['t_top'], 2),
                         round(sum(r['lev_ms']), 2)])
+    # the same batch with the symmetry fold (sym='auto', the reference CPU build's default): the same kept
+    # tree and values to rounding, fewer evaluations; reported beside the headline, not in it
+    fold_ms, fnev, fdiff, groups = 0.0, 0, 0.0, {}
+    if not args.no_fold:
+        L.sqb_l2_flush(256 << 20)
+        fres, fold_ms = sq.hsum_batch(jobs, workers=workers, device=local, sym='auto')
+        fnev = sum(r['nev'] for r in fres)
+        for j, fr, br in zip(jobs, fres, bres):
+            groups[j[0]] = fr['sym_order']
+            if br['S'][0] == br['S'][0] and br['S'][0] != 0:
+                fdiff = max(fdiff, abs(fr['S'][0] - br['S'][0])/abs(br['S'][0]))
     torch.cuda.synchronize()
     clk = clocks.stop()
-    mx, sm = reduce_max_sum([batch_ms, step_ms, wall], [lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches,
-                                                         h1[0].value - h0[0].value, h1[1].value - h0[1].value,
-                                                         0 if same else 1], world)
-    batch_ms, step_ms, wall = mx
-    lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches, h2d, d2h, ndiff = sm
+    mx, sm = reduce_max_sum([batch_ms, step_ms, wall, fold_ms, fdiff],
+                            [lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches, h1[0].value - h0[0].value,
+                             h1[1].value - h0[1].value, 0 if same else 1, fnev], world)
+    batch_ms, step_ms, wall, fold_ms, fdiff = mx
+    lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches, h2d, d2h, ndiff, fnev = sm
     if rank != 0:
         if world > 1:
             import torch.distributed as dist
@@ -500,6 +517,11 @@ def main():
         'batch': {'workers': workers, 'tuner_points_s': tune_rates, 'device_s': batch_ms*1e-3},
         'one_at_a_time': {'device_s': step_ms*1e-3, 'points_s': nev/(step_ms*1e-3),
                           'same_values_as_batch': ndiff == 0},
+        'fold': None if args.no_fold else {
+            'time_to_sum_s': fold_ms*1e-3, 'points': int(fnev), 'speedup_vs_unfolded': batch_ms/fold_ms,
+            'max_rel_diff_vs_unfolded': fdiff, 'group_orders': groups if world == 1 else None,
+            'note': 'the same concurrent batch with the symmetry fold found automatically (sym=auto); '
+                    'not the headline, whose point set is the unfolded tree'},
         'roofline': {'bound': 'fp64', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
                      'frac': achieved/peak if achieved else None, 'traffic': traffic,
                      'kernel': 'sqb_k_f64<graph> (FP64 evaluation), timed one integral at a time',

@@ -77,6 +77,13 @@ typedef struct {
                               nodes (g3_lbl) runs the FP64 pass of its level batches as passes over groups of
                               nodes (the same operations in the same order: the same values); 0 (default) = one
                               pass, measured faster on the B200 */
+    const char *sym;       /* SINCQED_SYM, the symmetry fold (driver/sum.c:21-26, 566-592): NULL, "0" or "off" = no
+                              fold (the default, and the reference's GPU build, whose point set is the unfolded
+                              tree); "auto" = find the group of axis permutations that leave the integrand
+                              invariant; "p0,p1,...[;q0,...]" = these involutions, each checked.  With a group the
+                              refinement levels evaluate only the children that are the minimum of their orbit,
+                              weight each by the orbit size and keep whole orbits: the kept tree is unchanged, the
+                              sums agree to rounding, and the evaluations drop by up to the group's order */
 } sqb_opts_t;
 #define SQB_CKPT_STOPPED 2 /* sqb_hsum's return code under ckpt_stop */
 
@@ -98,6 +105,13 @@ typedef struct {
      * number of FP64 launches; always: kernels of this library launched by the call */
     double f64_ms, dd_ms;
     long f64_launches, launches;
+    /* the symmetry fold: group order (1 = none), its generators as the reference prints them
+     * ("0,2,1,4,3; ..."), their largest deviation max|f(k) - f(k sigma)|/sum|terms| over 200 nodes, and
+     * the refused SINCQED_SYM entries (one per line) */
+    int sym_order;
+    char sym_desc[256];
+    double sym_worst;
+    char sym_msg[512];
 } sqb_result_t;
 
 void sqb_default_opts(sqb_opts_t *o);
@@ -124,6 +138,15 @@ int  sqb_hsum_batch(const sqb_job_t *jobs, int n, const sqb_opts_t *o, int worke
  * per second of device time; *best = the fastest candidate.  Returns 0 or a batch error. */
 int  sqb_batch_tune(const sqb_job_t *jobs, int n, const sqb_opts_t *o, const int *cand, int ncand, double *rate,
                     int *best);
+
+/* The symmetry fold's group search on its own (the part of driver/sum.c:464-592 that picks the group),
+ * with the caller's evaluator: fn(ctx, n, k, f, ab) puts f and the |.| sum of the integrand at the n
+ * lattice nodes k[i*D + d] (Sinc variables EX[k + K]) into f[i], ab[i] and returns 0.  spec as
+ * sqb_opts_t.sym.  Out: elems[e*12 + i] = image axis i of element e (element 0 the identity), desc,
+ * worst and msg as in sqb_result_t.  Returns the group order (1: no fold) or -1 if fn failed. */
+typedef int (*sqb_sym_eval_fn)(void *ctx, long n, const int *k, double *f, double *ab);
+int  sqb_sym_find(int D, sqb_sym_eval_fn fn, void *ctx, const char *spec, int *elems, char *desc, int ndesc,
+                  double *worst, char *msg, int nmsg);
 
 /* the graphs compiled into this library: name, Volkov string, L, D, mirror weight */
 int  sqb_graph_count(void);

@@ -262,6 +262,9 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     bat_o = os.path.join(OBJ, 'batch.o')
     if _newer(bat_o, [os.path.join(CSRC, 'batch.cpp')] + hdrs):
         jobs_list.append([CXX] + CXXFLAGS + ['-pthread', '-c', os.path.join(CSRC, 'batch.cpp'), '-o', bat_o])
+    sym_o = os.path.join(OBJ, 'sym.o')
+    if _newer(sym_o, [os.path.join(CSRC, 'sym.cpp')] + hdrs):
+        jobs_list.append([CXX] + CXXFLAGS + ['-c', os.path.join(CSRC, 'sym.cpp'), '-o', sym_o])
     n = jobs or min(len(jobs_list) or 1, os.cpu_count() or 4)
     if verbose and jobs_list:
         print('sincfeyn_b200: compiling %d objects with %d jobs' % (len(jobs_list), n), file=sys.stderr)
@@ -277,7 +280,7 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     with open(OCC, 'w') as f:
         json.dump(occ, f, indent=0, sort_keys=True)
     objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + \
-           [os.path.join(OBJ, 'kf_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o, bat_o, ck_o]
+           [os.path.join(OBJ, 'kf_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o, bat_o, ck_o, sym_o]
     if _newer(LIBSO, objs):
         _run([NVCC] + ARCH + ['-shared', '-o', LIBSO] + objs + ['-Xcompiler', '-fopenmp', '-lgomp', '-lpthread'])
     main_cpp = os.path.join(CSRC, 'main.cpp')

@@ -184,6 +184,17 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
 
 static inline double ddv(const double *x){ return x[0] + x[1]; }
 
+/* the fold's evaluator: f and the |.| sum at lattice nodes (lattice_node(), driver/lattice.c:30-34:
+ * sf = EX[k + K]) with the FP64 kernel that rounds as written (the reference's fd); nodes outside the
+ * lattice are clamped to its edge */
+extern "C" int sqb_eval_points_impl(const sqb_graph_t *g, long n, const double *sf, int prec, int ab, double *f, double *abs_);
+static int sym_nodes(void *ctx, long n, const int *k, double *f, double *ab){
+    const Run &R = *(const Run*)ctx;
+    std::vector<double> sf((size_t)n*R.D);
+    for(long i = 0; i < n*R.D; i++){ const int kk = k[i] < -R.K ? -R.K : (k[i] > R.K ? R.K : k[i]); sf[i] = R.X[kk + R.K]; }
+    return sqb_eval_points_impl(R.g, n, sf.data(), 0, 1, f, ab);
+}
+
 extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top, const sqb_opts_t *opts, sqb_result_t *res){
     memset(res, 0, sizeof *res);
     Run R; R.g = sqb_find_graph(graph);
@@ -202,6 +213,17 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
         else { R.X[k + K] = exp(k*h); R.Wt[k + K] = R.X[k + K]*h; }
     }
     if(sqb_dev_tables(R.X.data(), R.Wt.data(), K)) FAIL("device: %s", sqb_last_error());
+    /* the symmetry fold's group (driver/sum.c:566-592), before the run's clock starts as there */
+    sqb_sym_t sym; memset(&sym, 0, sizeof sym); sym.n = 1;
+    res->sym_order = 1;
+    if(R.o.sym && *R.o.sym){
+        static thread_local int el[SQB_SYMG*SQB_MAXD];
+        const int n = sqb_sym_find(R.D, sym_nodes, &R, R.o.sym, el, res->sym_desc, sizeof res->sym_desc, &res->sym_worst,
+                                   res->sym_msg, sizeof res->sym_msg);
+        if(n < 0) FAIL("symmetry search: device: %s", sqb_last_error());
+        sym.n = n; res->sym_order = n;
+        for(int e = 0; e < n; e++) for(int i = 0; i < SQB_MAXD; i++) sym.g[e][i] = (signed char)el[e*SQB_MAXD + i];
+    }
     double t0 = now();
     const unsigned long long l0 = sqb_launch_count() + sqb_top_launches();
     { double a, b; long c; sqb_kernel_times(&a, &b, &c, 1); }
@@ -265,6 +287,7 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
         sqb_level_t L; memset(&L, 0, sizeof L);
         L.g = R.g; L.cells = dcur + c0; L.ncell = ncur - c0; L.st = st; L.last = last;
         L.pw = pow(st, R.D); L.thr = eps*res->ref*1e-2; L.t = R.t; L.max_children = R.o.max_children;
+        L.sym = &sym;
         if(!last){
             double want = (double)(ncur - c0)*(double)(1L << R.D) + nkeep0;
             double room = 0.35*MEMSHARE*(double)sqb_dev_total_bytes()/sizeof(sqb_pt_t);
@@ -330,7 +353,6 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
 }
 
 /* pointwise kernel evaluation for parity checks */
-extern "C" int sqb_eval_points_impl(const sqb_graph_t *g, long n, const double *sf, int prec, int ab, double *f, double *abs_);
 extern "C" int sqb_eval_points(const char *graph, long n, const double *sf, int prec, int ab, double *f, double *abs_){
     const sqb_graph_t *g = sqb_find_graph(graph);
     if(!g) FAIL("no graph %s in this build", graph);

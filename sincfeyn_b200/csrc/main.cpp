@@ -69,6 +69,7 @@ int main(int argc, char **argv){
     if((e = getenv("SQB_VERBOSE"))) o.verbose = atoi(e);
     if((e = getenv("SQB_FMA"))) o.fma = atoi(e);
     if((e = getenv("SQB_SPLIT"))) o.split = atoi(e);
+    o.sym = getenv("SINCQED_SYM");     /* unset: no fold, as the reference's GPU build (driver/sum.c:571) */
     /* checkpoints at every level end, on by default as in the reference (driver/main.c:28,184) */
     o.ckpt_every = 600;
     if((e = getenv("SINCQED_CKPT"))) o.ckpt_every = atof(e);
@@ -126,6 +127,13 @@ int main(int argc, char **argv){
         const int L = info[0], D = info[1], w = info[2]; const char *volkov = sqb_graph_volkov(name);
         sqb_result_t R;
         if(sqb_hsum(name, h, N, eps, top, &o, &R)){ fprintf(stderr, "sincqed: %s: %s\n", name, sqb_error()); rc = 2; continue; }
+        for(const char *m = R.sym_msg; *m; ){
+            const char *nl = strchr(m, '\n'); const int len = nl ? (int)(nl - m) : (int)strlen(m);
+            say("# %s: %.*s\n", name, len, m); m += len + (nl ? 1 : 0);
+        }
+        if(R.sym_order > 1)
+            say("# %s: symmetry fold sigma=%s (group of order %d), max |f(k)-f(k sigma)|/sum|terms| over 200 nodes %.1e\n",
+                name, R.sym_desc, R.sym_order, R.sym_worst);
         if(R.zero) say("# %s: integrand is exactly zero at 4097 probe nodes; reported as zero without a scan\n", name);
         const double v = w*R.S[0], d2 = fabs(R.S[1] - R.S[0]);
         const double disc = R.Ah > 0 ? 2*d2*d2/R.Ah : 0;

@@ -23,6 +23,7 @@
 #include "sqb_rt.h"
 #include "sqdd.cuh"
 #include <atomic>
+#include <vector>
 #include "sincfeyn_b200.h"
 
 extern "C" const sqb_graph_t *const SQB_ALL[];
@@ -62,6 +63,7 @@ typedef struct {
     double pw, thr;
     const double *v, *uu;
     const unsigned char *stt;
+    sqb_sym_t sym;                /* the symmetry fold (sym.n <= 1: off) */
 } lvl_t;
 
 struct Dev {
@@ -329,6 +331,32 @@ extern "C" void sqb_kernel_times(double *f64_ms, double *dd_ms, long *f64_launch
 __device__ __forceinline__ sqdd shfl_dd(const sqdd &a, int off){
     return sqdd(__shfl_down_sync(0xffffffffu, a.hi, off), __shfl_down_sync(0xffffffffu, a.lo, off));
 }
+/* child i's coordinates k_d - st bit_d(b) (driver/sum.c:407) */
+__device__ __forceinline__ void child_of(const lvl_t &a, long i, int *k){
+    const long c = i >> a.D; const int b = (int)(i & ((1L << a.D) - 1));
+    const signed char *p = a.cells + c*SQB_MAXD;
+    for(int d = 0; d < a.D; d++) k[d] = p[d] - (((b >> d) & 1) ? a.st : 0);
+}
+/* the image of k under group element e (symimg(), driver/sum.c:29) is k'_i = k[g[e][i]]; 0 if k is not
+ * the minimum of its orbit, else the orbit size (symw(), driver/sum.c:30-37) */
+__device__ int orbit_size(const sqb_sym_t &s, const int *k, int D){
+    int stab = 1;
+    for(int e = 1; e < s.n; e++){
+        int c = 0;
+        for(int i = 0; i < D && !c; i++){ const int x = k[i], y = k[s.g[e][i]]; if(x != y) c = x < y ? -1 : 1; }
+        if(c > 0) return 0;
+        if(!c) stab++;
+    }
+    return s.n/stab;
+}
+/* a present child's multiplicity: its orbit size under a fold, else 1 */
+__device__ __forceinline__ int child_weight(const lvl_t &a, long i){
+    if(a.sym.n <= 1) return 1;
+    int k[SQB_MAXD];
+    child_of(a, i, k);
+    return orbit_size(a.sym, k, a.D);
+}
+
 __device__ __forceinline__ int parent_tier(const lvl_t &a, long i){
     const long c = i >> a.D;
     return (a.cells[c*SQB_MAXD + SQB_PFLAG] >> 1) & 3;
@@ -350,8 +378,10 @@ __global__ void __launch_bounds__(RT) sqb_k_reduce(const lvl_t a, part_t *bp, un
         if(i >= a.n) break;
         const unsigned char s = a.stt[i];
         if(!(s & SQB_PRESENT)) continue;
-        const double v = a.v[i], vp = v*a.pw, av = fabs(v);
-        S = sqdd_add_d(S, vp); A += av; ne++;
+        /* a folded point stands for its orbit: (mw v) pw and mw |v| (driver/sum.c:734-745) */
+        const int mw = child_weight(a, i);
+        const double m = (double)mw, v = a.v[i], vp = (m*v)*a.pw, av = fabs(v);
+        S = sqdd_add_d(S, vp); A += m*av; ne++;
         nsk += (s & SQB_SKIPPED) ? 1 : 0;
         if(s & SQB_FALLBACK){ nq++; uu += a.uu[i]; }
         if(s & SQB_UNRES) nu++;
@@ -359,8 +389,8 @@ __global__ void __launch_bounds__(RT) sqb_k_reduce(const lvl_t a, part_t *bp, un
             const int te = parent_tier(a, i);
             if(te >= 1) b1 = sqdd_add_d(b1, vp);
             if(te >= 2) b2 = sqdd_add_d(b2, vp);
-        } else if(av >= a.thr) keep++;
-        else dr += av*a.pw;
+        } else if(av >= a.thr) keep += mw;
+        else dr += (m*av)*a.pw;
     }
     sqdd Ad(A), dd(dr), ud(uu);
     for(int off = 16; off; off >>= 1){
@@ -455,7 +485,7 @@ __global__ void __launch_bounds__(RT) sqb_k_scatter(const lvl_t a, const unsigne
     for(int j = 0; j < RPT; j++){
         const long i = t0 + j;
         if(i >= a.n) break;
-        if((a.stt[i] & SQB_PRESENT) && fabs(a.v[i]) >= a.thr){ mask |= 1u << j; cnt++; }
+        if((a.stt[i] & SQB_PRESENT) && fabs(a.v[i]) >= a.thr){ mask |= 1u << j; cnt += child_weight(a, i); }
     }
     /* block exclusive scan of cnt */
     __shared__ int ws[RT/32];
@@ -471,20 +501,35 @@ __global__ void __launch_bounds__(RT) sqb_k_scatter(const lvl_t a, const unsigne
     for(int j = 0; j < RPT; j++){
         if(!(mask >> j & 1)) continue;
         const long i = t0 + j;
-        if((long)o >= cap){ atomicAdd(overflow, 1ULL); o++; continue; }
-        const long c = i >> a.D; const int b = (int)(i & ((1L << a.D) - 1));
+        const long c = i >> a.D;
         const signed char *p = a.cells + c*SQB_MAXD;
         const unsigned char s = a.stt[i];
         const double av = fabs(a.v[i]);
         const int te = (p[SQB_PFLAG] >> 1) & 3, tv = (av >= thr10) + (av >= thr100);
         const int psk = (s & SQB_SKIPPED) ? 1 : 0, nr = (s & SQB_NEAR) ? 1 : 0;
-        union { signed char k[SQB_MAXD]; int w[3]; } q;
-        q.w[0] = q.w[1] = q.w[2] = 0;
-        for(int d = 0; d < a.D; d++) q.k[d] = (signed char)(p[d] - (((b >> d) & 1) ? a.st : 0));
-        q.k[SQB_PFLAG] = (signed char)((a.abskip && (psk || !nr)) | ((te < tv ? te : tv) << 1));
-        int *dst = (int*)(next + o);
-        dst[0] = q.w[0]; dst[1] = q.w[1]; dst[2] = q.w[2];
-        o++;
+        const signed char fl = (signed char)((a.abskip && (psk || !nr)) | ((te < tv ? te : tv) << 1));
+        int k[SQB_MAXD];
+        child_of(a, i, k);
+        /* the child, then (under a fold) the other members of its orbit in group order, each once
+         * (symorbit(), driver/sum.c:38-46), all with the child's flags (driver/sum.c:741-744) */
+        const int ng = a.sym.n > 1 ? a.sym.n : 1;
+        for(int e = 0; e < ng; e++){
+            bool dup = false;
+            for(int f = 0; f < e && !dup; f++){
+                bool eq = true;
+                for(int d = 0; d < a.D && eq; d++) eq = k[a.sym.g[e][d]] == k[a.sym.g[f][d]];
+                dup = eq;
+            }
+            if(dup) continue;
+            if((long)o >= cap){ atomicAdd(overflow, 1ULL); o++; continue; }
+            union { signed char k[SQB_MAXD]; int w[3]; } q;
+            q.w[0] = q.w[1] = q.w[2] = 0;
+            for(int d = 0; d < a.D; d++) q.k[d] = (signed char)(e ? k[a.sym.g[e][d]] : k[d]);
+            q.k[SQB_PFLAG] = fl;
+            int *dst = (int*)(next + o);
+            dst[0] = q.w[0]; dst[1] = q.w[1]; dst[2] = q.w[2];
+            o++;
+        }
     }
 }
 
@@ -501,6 +546,7 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
         const sqb_pt_t *cells = L->cells + c0;
         sqb_eval_t a; memset(&a, 0, sizeof a); fill_eval(&a, &L->t);
         a.pts = cells; a.n = nc; a.esize = 1; a.stride = SQB_MAXD; a.flag_at = SQB_PFLAG; a.cells = 1; a.st = L->st;
+        if(L->sym && L->sym->n > 1) a.sym = *L->sym;
         /* level mode: the FP64 pass sums the tiles without fallback points (the all-dd form has no FP64
          * pass: the reduce kernel sums every tile) */
         int can = 0;
@@ -510,6 +556,7 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
         if(eval_batch(g, &a, &L->t, nch)) return -1;
         lvl_t r; r.cells = (const signed char*)cells; r.n = nch; r.D = D; r.st = L->st; r.last = L->last;
         r.abskip = L->t.abskip; r.pw = L->pw; r.thr = L->thr; r.v = G.v; r.uu = G.uu; r.stt = G.stt;
+        r.sym = a.sym;
         const long nb = (nch + RTILE - 1)/RTILE;
         sqb_k_reduce<<<(unsigned)nb, RT, 0, G.s>>>(r, G.bp, G.bkeep, fused ? G.tfb : NULL);
         CKR(cudaGetLastError());
@@ -670,37 +717,42 @@ extern "C" void sqb_gg_launch(const sqb_graph_t *g, void *st, long n, const shor
 extern "C" int sqb_eval_points_impl(const sqb_graph_t *g, long n, const double *sf, int prec, int ab, double *f, double *abs_){
     if(n <= 0) return 0;
     const int D = g->D;
-    double *dsf = NULL, *dv = NULL, *dab = NULL, *dvl = NULL, *dabl = NULL; unsigned char *dsk = NULL;
-    CKR(cudaMalloc(&dsf, n*D*sizeof(double))); CKR(cudaMalloc(&dv, n*sizeof(double))); CKR(cudaMalloc(&dab, n*sizeof(double)));
-    CKR(cudaMalloc(&dvl, n*sizeof(double))); CKR(cudaMalloc(&dabl, n*sizeof(double))); CKR(cudaMalloc(&dsk, n));
-    CKR(cudaMemcpy(dsf, sf, n*D*sizeof(double), cudaMemcpyHostToDevice));
-    CKR(cudaMemset(dsk, ab ? 0 : 1, n));
-    double one = 1.0, *dX = NULL; CKR(cudaMalloc(&dX, sizeof(double))); CKR(cudaMemcpy(dX, &one, sizeof one, cudaMemcpyHostToDevice));
+    /* one stream-ordered block (no device-wide synchronisation, so other threads' work runs on):
+     * sf[n D], v, ab, vlo, ablo [n each], X = 1, skip[n] */
+    const size_t nd = (size_t)n*D + 4*(size_t)n + 1;
+    char *blk = NULL;
+    CKR(cudaMallocAsync((void**)&blk, nd*sizeof(double) + (size_t)n, G.s));
+    double *dsf = (double*)blk, *dv = dsf + (size_t)n*D, *dab = dv + n, *dvl = dab + n, *dabl = dvl + n, *dX = dabl + n;
+    unsigned char *dsk = (unsigned char*)(dX + 1);
+    const double one = 1.0;
+    CKR(cudaMemcpyAsync(dsf, sf, (size_t)n*D*sizeof(double), cudaMemcpyHostToDevice, G.s));
+    CKR(cudaMemcpyAsync(dX, &one, sizeof one, cudaMemcpyHostToDevice, G.s));
+    CKR(cudaMemsetAsync(dsk, ab ? 0 : 1, n, G.s));
     sqb_eval_t a; memset(&a, 0, sizeof a);
     a.pts = NULL; a.n = n; a.esize = 1; a.stride = D; a.flag_at = -1; a.cells = 0;
     a.X = dX; a.Wt = dX; a.K = 0; a.raw = 1; a.skip = dsk; a.v = dv; a.ab = dab; a.sfin = dsf; a.vlo = dvl; a.ablo = dabl;
     size_t smem = 2*sizeof(double);
+    int rc = 0;
     if(prec == 0 || prec == 2){
         const int w = f64_which(g, prec == 2);
-        if(prec == 2 && w != 2){ snprintf(g_err, sizeof g_err, "%s: no contracted FP64 kernel in this library", g->name); return -1; }
-        launch_f64(g, w, &a, grid_for(g, w, n, smem), smem, G.s);
+        if(prec == 2 && w != 2){ snprintf(g_err, sizeof g_err, "%s: no contracted FP64 kernel in this library", g->name); rc = -1; }
+        else launch_f64(g, w, &a, grid_for(g, w, n, smem), smem, G.s);
     } else { sqb_dd_t d; memset(&d, 0, sizeof d); d.e = a; d.all = 1; d.uu = dvl; g->dd(&d, grid_for(g, 1, n, smem), 128, smem, G.s); }
-    CKR(cudaGetLastError());
-    CKR(cudaStreamSynchronize(G.s));
-    if(prec == 0 || prec == 2){
-        CKR(cudaMemcpy(f, dv, n*sizeof(double), cudaMemcpyDeviceToHost));
-        CKR(cudaMemcpy(abs_, dab, n*sizeof(double), cudaMemcpyDeviceToHost));
-    } else {
-        double *h = (double*)malloc(4*n*sizeof(double));
-        CKR(cudaMemcpy(h, dv, n*sizeof(double), cudaMemcpyDeviceToHost));
-        CKR(cudaMemcpy(h + n, dvl, n*sizeof(double), cudaMemcpyDeviceToHost));
-        CKR(cudaMemcpy(h + 2*n, dab, n*sizeof(double), cudaMemcpyDeviceToHost));
-        CKR(cudaMemcpy(h + 3*n, dabl, n*sizeof(double), cudaMemcpyDeviceToHost));
-        for(long i = 0; i < n; i++){ f[2*i] = h[i]; f[2*i + 1] = h[n + i]; abs_[2*i] = h[2*n + i]; abs_[2*i + 1] = h[3*n + i]; }
-        free(h);
+    if(!rc){
+        CKR(cudaGetLastError());
+        if(prec == 0 || prec == 2){
+            CKR(cudaMemcpyAsync(f, dv, n*sizeof(double), cudaMemcpyDeviceToHost, G.s));
+            CKR(cudaMemcpyAsync(abs_, dab, n*sizeof(double), cudaMemcpyDeviceToHost, G.s));
+            CKR(cudaStreamSynchronize(G.s));
+        } else {
+            std::vector<double> h(4*(size_t)n);
+            CKR(cudaMemcpyAsync(h.data(), dv, 4*n*sizeof(double), cudaMemcpyDeviceToHost, G.s));   /* v, ab, vlo, ablo */
+            CKR(cudaStreamSynchronize(G.s));
+            for(long i = 0; i < n; i++){ f[2*i] = h[i]; f[2*i + 1] = h[2*n + i]; abs_[2*i] = h[n + i]; abs_[2*i + 1] = h[3*n + i]; }
+        }
     }
-    cudaFree(dsf); cudaFree(dv); cudaFree(dab); cudaFree(dvl); cudaFree(dabl); cudaFree(dsk); cudaFree(dX);
-    return 0;
+    cudaFreeAsync(blk, G.s);
+    return rc;
 }
 
 /* FP64 peak probe: independent chains of fused multiply-adds (8 per thread, unrolled) or of adds, on

@@ -16,6 +16,16 @@ enum {
     SQB_SKIPPED = 16      /* evaluated without the |.| sums (driver/eval.c:35) */
 };
 
+/* A group of axis permutations under which the integrand is invariant (the symmetry fold of
+ * driver/sum.c:21-46): n elements, g[0] the identity, image of k under element e: k'_i = k[g[e][i]].
+ * n <= 1: no fold.  With a group, a level batch evaluates only the children that are the lexicographic
+ * minimum of their orbit, weights each by the orbit size and keeps the whole orbit. */
+#define SQB_SYMG 64
+typedef struct {
+    int n;
+    signed char g[SQB_SYMG][12];
+} sqb_sym_t;
+
 /* One launch of the FP64 evaluation kernel over nodes, or over the 2^D children of cells.
  * Coordinates are integers k (|k| <= K) of esize bytes (1: the pt_t layout of the level lists and
  * checkpoints, 2: the int16 layout of the reference's GPU plug-in), stride elements per node or
@@ -55,6 +65,7 @@ typedef struct {
     unsigned char *tfb;
     double pw, thr;               /* the level's weight step^D and keep threshold */
     int last;                     /* the last level: shadow-tier sums, no kept children */
+    sqb_sym_t sym;                /* cells only: the symmetry fold (sym.n <= 1: off) */
 } sqb_eval_t;
 
 /* The double-double kernel over a list of points of the same launch geometry (fb/nfb from the FP64

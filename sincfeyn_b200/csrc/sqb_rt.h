@@ -53,6 +53,7 @@ typedef struct {
     double pw, thr;
     sqb_test_t t;
     long max_children;                  /* children per batch (0: default) */
+    const sqb_sym_t *sym;               /* the symmetry fold (NULL or n <= 1: off) */
 } sqb_level_t;
 int  sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n, double *ms);
 

@@ -47,10 +47,34 @@
 #endif
 #define SQB_QEPS 4.93e-32   /* double-double epsilon of the fallback's error model (driver/common.h:8) */
 
-/* coordinates and weight of point i; returns false for a child below the box */
+/* The symmetry fold's test (symw(), driver/sum.c:30-37): 0 if k is not the lexicographic minimum of
+ * its orbit under the group, else the orbit size n / |stabiliser|.  The image k[g[e][i]] is selected
+ * from the registers by an unrolled compare, so k stays out of local memory. */
 template<int D>
-__device__ __forceinline__ bool sqb_point(const sqb_eval_t &a, const double *sX, const double *sW,
-                                          long i, long *cell, double *sf, double *w){
+__device__ __forceinline__ int sqb_orbit(const sqb_sym_t &s, const int (&k)[D]){
+    int stab = 1;
+    for(int e = 1; e < s.n; e++){
+        int c = 0;
+#pragma unroll
+        for(int i = 0; i < D; i++){
+            const int p = s.g[e][i];
+            int y = k[0];
+#pragma unroll
+            for(int j = 1; j < D; j++) y = p == j ? k[j] : y;
+            if(c == 0 && k[i] != y) c = k[i] < y ? -1 : 1;
+        }
+        if(c > 0) return 0;
+        if(c == 0) stab++;
+    }
+    return s.n/stab;
+}
+
+/* coordinates and weight of point i; returns 0 for a child below the box or, under a symmetry fold, a
+ * child that is not the minimum of its orbit (driver/sum.c:405-409), else the point's multiplicity
+ * (the orbit size; 1 without a fold) */
+template<int D>
+__device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const double *sX, const double *sW,
+                                         long i, long *cell, double *sf, double *w){
     long c; int b;
     if(a.cells){ c = i >> D; b = (int)(i & ((1L << D) - 1)); } else { c = i; b = 0; }
     *cell = c;
@@ -58,14 +82,16 @@ __device__ __forceinline__ bool sqb_point(const sqb_eval_t &a, const double *sX,
 #pragma unroll
         for(int d = 0; d < D; d++) sf[d] = a.sfin[i*D + d];
         *w = 1.0;
-        return true;
+        return 1;
     }
     double ww = 1.0; bool in = true;
+    int kk[D];
     if(a.esize == 1){
         const signed char *p = (const signed char*)a.pts + c*(long)a.stride;
 #pragma unroll
         for(int d = 0; d < D; d++){
             int kd = p[d] - (((b >> d) & 1) ? a.st : 0);
+            kk[d] = kd;
             if(kd < -a.K){ in = false; kd = -a.K; }
             sf[d] = sX[kd + a.K]; ww = ww*sW[kd + a.K];
         }
@@ -74,12 +100,14 @@ __device__ __forceinline__ bool sqb_point(const sqb_eval_t &a, const double *sX,
 #pragma unroll
         for(int d = 0; d < D; d++){
             int kd = p[d] - (((b >> d) & 1) ? a.st : 0);
+            kk[d] = kd;
             if(kd < -a.K){ in = false; kd = -a.K; }
             sf[d] = sX[kd + a.K]; ww = ww*sW[kd + a.K];
         }
     }
     *w = ww;
-    return in;
+    if(!in) return 0;
+    return a.cells && a.sym.n > 1 ? sqb_orbit<D>(a.sym, kk) : 1;
 }
 
 template<int D>
@@ -198,8 +226,8 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const sqb_eval_
             const long i = tile*tl + (long)j*SQB_BLOCK + t;
             if(i >= n) break;
             long c; double sf[D], w;
-            const bool in = sqb_point<D>(a, sX, sW, i, &c, sf, &w);
-            if(!in){
+            const int mw = sqb_point<D>(a, sX, sW, i, &c, sf, &w);
+            if(!mw){
                 a.v[i] = 0;
                 if(a.raw) a.ab[i] = 0; else a.stt[i] = 0;
                 continue;
@@ -216,14 +244,15 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const sqb_eval_
 #if SQB_FUSE
             if(lvl){
                 if(fallback){ ta.fb = 1; continue; }
-                const double vp = v*a.pw, av = fabs(v);
-                sqb_acc_dd(ta.S, t, vp); ta.A[t] += av; ta.ne[t]++; ta.nsk[t] += sk ? 1 : 0;
+                /* a folded point stands for its orbit: (mw v) pw and mw |v| (driver/sum.c:734-745) */
+                const double m = (double)mw, vp = (m*v)*a.pw, av = fabs(v);
+                sqb_acc_dd(ta.S, t, vp); ta.A[t] += m*av; ta.ne[t]++; ta.nsk[t] += sk ? 1 : 0;
                 if(a.last){
                     const int te = (((const signed char*)a.pts)[c*(long)a.stride + a.flag_at] >> 1) & 3;
                     if(te >= 1) sqb_acc_dd(ta.b1, t, vp);
                     if(te >= 2) sqb_acc_dd(ta.b2, t, vp);
-                } else if(av >= a.thr) ta.keep[t]++;
-                else ta.dr[t] += av*a.pw;
+                } else if(av >= a.thr) ta.keep[t] += mw;
+                else ta.dr[t] += (m*av)*a.pw;
             }
 #else
             (void)fallback;

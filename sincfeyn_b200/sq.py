@@ -24,7 +24,7 @@ class Opts(C.Structure):
                 ('abskip', C.c_int), ('abcheck', C.c_int), ('dropunres', C.c_int), ('growskip', C.c_int),
                 ('alldd', C.c_int), ('device', C.c_int), ('max_children', C.c_long), ('verbose', C.c_int),
                 ('ckpt_every', C.c_double), ('ckpt_dir', C.c_char_p), ('ckpt_stop', C.c_int), ('fma', C.c_int),
-                ('split', C.c_int)]
+                ('split', C.c_int), ('sym', C.c_char_p)]
 
 
 class Result(C.Structure):
@@ -36,7 +36,9 @@ class Result(C.Structure):
                 ('abskipped', C.c_long), ('unresdrop', C.c_long), ('zero', C.c_int),
                 ('t_top', C.c_double), ('t_levels', C.c_double), ('nlev', C.c_int),
                 ('lev_evals', C.c_long * 16), ('lev_ms', C.c_double * 16),
-                ('f64_ms', C.c_double), ('dd_ms', C.c_double), ('f64_launches', C.c_long), ('launches', C.c_long)]
+                ('f64_ms', C.c_double), ('dd_ms', C.c_double), ('f64_launches', C.c_long), ('launches', C.c_long),
+                ('sym_order', C.c_int), ('sym_desc', C.c_char * 256), ('sym_worst', C.c_double),
+                ('sym_msg', C.c_char * 512)]
 
 
 class Job(C.Structure):
@@ -47,6 +49,11 @@ class Job(C.Structure):
 
 class SqbError(RuntimeError):
     pass
+
+
+# sqb_sym_eval_fn: (ctx, n, k[n*D], f[n], ab[n]) -> 0
+SYM_EVAL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_long, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                          C.POINTER(C.c_double))
 
 
 def lib():
@@ -79,6 +86,9 @@ def lib():
                                      C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.sqb_batch_tune.argtypes = [C.POINTER(Job), C.c_int, C.POINTER(Opts), C.POINTER(C.c_int), C.c_int,
                                      C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.sqb_sym_find.argtypes = [C.c_int, SYM_EVAL_FN, C.c_void_p, C.c_char_p, C.POINTER(C.c_int), C.c_char_p,
+                                   C.c_int, C.POINTER(C.c_double), C.c_char_p, C.c_int]
+        L.sqb_sym_find.restype = C.c_int
         _lib = L
     return _lib
 
@@ -195,6 +205,8 @@ def hsum(graph, h, N, eps, top=-1, **opts):
 
 def _result_dict(r):
     d = {f: getattr(r, f) for f, _ in Result._fields_}
+    d['sym_desc'] = r.sym_desc.decode()
+    d['sym_msg'] = r.sym_msg.decode()
     d['S'] = list(r.S)
     d['lev_evals'] = list(r.lev_evals)[:r.nlev]
     d['lev_ms'] = list(r.lev_ms)[:r.nlev]
@@ -278,6 +290,35 @@ def run(h, N, eps, selectors, top=-1, **opts):
                          prune=w * r['prune'], trunc=w * r['trunc'], round=w * r['unres'],
                          S_2h=w * S1, evals=r['nev'], quad=r['nq'], kept=r['kept_top'], time=r['t'], raw=r))
     return rows
+
+
+def sym_find(D, evaluate, spec='auto'):
+    """The symmetry fold's group search (sqb_sym_find) with a Python evaluator: evaluate(k) takes an
+    (n, D) int array of lattice nodes and returns (f, ab) arrays of n values.  spec as Opts.sym.
+    Returns dict(order, elems (order x D), desc, worst, msg)."""
+    err = []
+
+    def cb(_ctx, n, k, f, ab):
+        try:
+            kk = np.ctypeslib.as_array(k, shape=(n * D,)).reshape(n, D).copy()
+            fv, av = evaluate(kk)
+            np.ctypeslib.as_array(f, shape=(n,))[:] = fv
+            np.ctypeslib.as_array(ab, shape=(n,))[:] = av
+            return 0
+        except Exception as e:  # reported after the call
+            err.append(e)
+            return -1
+    fn = SYM_EVAL_FN(cb)
+    el = (C.c_int * (64 * 12))()
+    desc = C.create_string_buffer(1024)
+    msg = C.create_string_buffer(2048)
+    worst = C.c_double()
+    n = lib().sqb_sym_find(int(D), fn, None, spec.encode() if spec else None, el, desc, len(desc), C.byref(worst),
+                           msg, len(msg))
+    if n < 0:
+        raise SqbError('symmetry search failed: %r' % (err[0] if err else 'evaluator'))
+    elems = np.array(el[:], dtype=np.int64).reshape(64, 12)[:n, :D]
+    return dict(order=n, elems=elems, desc=desc.value.decode(), worst=worst.value, msg=msg.value.decode())
 
 
 def eval_points(graph, sf, prec=0, ab=1):

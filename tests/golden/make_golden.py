@@ -21,8 +21,13 @@ Fixtures
   synth_runs.json               the reference's hsum() on the synthetic integrands, -ffp-contract=off build,
                                 SINCQED_SYM=0 and SINCQED_KEEPBT=1 (one boundary table, the exact grow):
                                 syn_d5 at h = 1.0 (N = 61) and h = 0.7 (N = 87), syn_d8 at h = 1.0 (N = 61)
+  fold.json                     the symmetry fold (driver/sum.c:21-46, 464-592), -ffp-contract=off build:
+                                the group line the reference prints for every graph of g2 g3 v3 v4 w4
+                                (`run 2.0 13 1e-4 GRAPH`, SINCQED_SYM unset = auto; the search's nodes only
+                                need K >= 6), and folded sums (SINCQED_SYM unset, SINCQED_KEEPBT=1) with
+                                top = 2 so that kept orbits go on to a second refinement level
 
-    python tests/golden/make_golden.py [all2 boxsum pointwise synth]   # default: all of them
+    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold]   # default: all of them
 """
 import json
 import os
@@ -108,8 +113,33 @@ def synth():
         json.dump(d, f, indent=1)
 
 
+FOLD_GROUP_RUN = (2.0, 13, 1e-4)
+FOLD_RUNS = [('v2_00', 1.0, 97, 2), ('g3_07', 1.0, 97, 2), ('g3_25', 1.0, 97, 2), ('g3_08', 1.0, 97, 2),
+             ('v3_00', 1.0, 97, 2), ('v3_03', 1.0, 97, 2), ('v3_p4Vm', 1.0, 97, 2), ('g3_lbl', 1.5, 65, 2)]
+_SYMLINE = re.compile(r'^# (\S+): symmetry fold sigma=(.*) \(group of order (\d+)\), '
+                      r'max \|f\(k\)-f\(k sigma\)\|/sum\|terms\| over 200 nodes (\S+)$', re.M)
+
+
+def fold():
+    h, N, eps = FOLD_GROUP_RUN
+    d = {'group_run': {'h': h, 'N': N, 'eps': eps}, 'groups': {}, 'runs': [], 'env': {'SINCQED_KEEPBT': '1'}}
+    names = [n for n in refpy.names() if n.split('_')[0] in ('g2', 'v2', 'g3', 'v3', 'w3', 'v4', 'w4')]
+    for i in range(0, len(names), 16):
+        _, out = refpy.run(refpy.SINCQED_EXACT, h, N, eps, names[i:i + 16])
+        for m in _SYMLINE.finditer(out):
+            d['groups'][m.group(1)] = {'desc': m.group(2), 'order': int(m.group(3)), 'worst': m.group(4)}
+    d['searched'] = names
+    for name, h, N, top in FOLD_RUNS:
+        rows, out = refpy.run(refpy.SINCQED_EXACT, h, N, 1e-12, [name], top=top, env=d['env'])
+        r = with_log(rows, out)[0]
+        r.pop('time_s', None)
+        d['runs'].append(r)
+    with open(os.path.join(OUT, 'fold.json'), 'w') as f:
+        json.dump(d, f, indent=1)
+
+
 if __name__ == '__main__':
-    parts = sys.argv[1:] or ['all2', 'boxsum', 'pointwise', 'synth']
+    parts = sys.argv[1:] or ['all2', 'boxsum', 'pointwise', 'synth', 'fold']
     if 'all2' in parts:
         all2()
     if 'boxsum' in parts:
@@ -122,3 +152,5 @@ if __name__ == '__main__':
         pointwise('w4', ('w4_',), 32)
     if 'synth' in parts:
         synth()
+    if 'fold' in parts:
+        fold()
