@@ -412,7 +412,9 @@ def main():
     import ctypes as C
     L.sqb_timer_stop.restype = C.c_double
     L.sqb_l2_flush.argtypes = [C.c_size_t]
-    sq.kernel_timing(True)
+    # the batch runs without per-kernel events (they synchronise the host once per level batch); the
+    # one-at-a-time pass below turns them on for the roofline
+    sq.kernel_timing(False)
     # the device code of every graph of the set is loaded before the timed region (CUDA loads a kernel
     # on its first launch otherwise); the one-time cost is reported as load_s
     t_load = time.perf_counter()
@@ -451,6 +453,7 @@ def main():
     bvals = {j[0]: r['S'][0] for j, r in zip(jobs, bres)}
     # the same integrals one at a time, each kernel timed alone: the level-pass throughput and the FP64
     # roofline (a kernel that shares the device with other streams would read slow)
+    sq.kernel_timing(True)
     step_ms, lev_ms, lev_ev, f64_ms, f64_n, fl, results, same = 0.0, 0.0, 0, 0.0, 0, 0.0, [], True
     for g in mine:
         L.sqb_l2_flush(256 << 20)
@@ -470,6 +473,7 @@ def main():
     # the same batch with the symmetry fold (sym='auto', the reference CPU build's default): the same kept
     # tree and values to rounding, fewer evaluations; reported beside the headline, not in it
     fold_ms, fnev, fdiff, groups = 0.0, 0, 0.0, {}
+    sq.kernel_timing(False)
     if not args.no_fold:
         L.sqb_l2_flush(256 << 20)
         fres, fold_ms = sq.hsum_batch(jobs, workers=workers, device=local, sym='auto')

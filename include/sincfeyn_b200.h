@@ -170,10 +170,10 @@ const char *sqb_device_info(void);
  * kernels loaded, or -1 */
 int  sqb_preload(const char *graph);
 
-/* instrumentation: bracket every FP64 and double-double evaluation launch with events (one
- * synchronisation per batch) so that sqb_result_t carries their times; and the measured FP64 rate of
- * this device in TFLOP/s (fma = 1: fused multiply-adds, 2 flops each; 0: adds), the roofline
- * denominator of the evaluation kernels */
+/* instrumentation: bracket every FP64 and double-double evaluation launch with events (read when the
+ * call next waits on its stream, no extra synchronisation) so that sqb_result_t carries their times; and
+ * the measured FP64 rate of this device in TFLOP/s (fma = 1: fused multiply-adds, 2 flops each; 0: adds),
+ * the roofline denominator of the evaluation kernels */
 void sqb_kernel_timing(int on);
 double sqb_probe_fp64(int fma, long iters);
 /* bytes copied host->device and device->host by the chosen form so far */

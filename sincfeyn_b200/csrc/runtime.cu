@@ -70,7 +70,7 @@ struct Dev {
     int on, dev, nsm;
     cudaEvent_t t0, t1; void *flush; size_t flushn;
     unsigned long long launches;   /* kernels of this library launched so far */
-    cudaEvent_t k0, k1, d1;
+    cudaEvent_t kev[3*256]; int nkev, kevn;   /* kernel timing: (FP64 start, FP64 end / dd start, dd end) per pass */
     double f64_ms, dd_ms; long f64_n;
     char info[256];
     cudaStream_t s;
@@ -88,6 +88,30 @@ static thread_local Dev G;
 static int KTIME;                  /* sqb_kernel_timing(): all threads */
 static std::atomic<unsigned long long> H2D, D2H;   /* bytes copied by the chosen form's calls, all threads */
 
+/* the timed passes so far: their events are read once the stream has passed them (the callers that wait
+ * on the stream anyway), so timing adds no synchronisation between a level's batches */
+static void ktime_collect(void){
+    if(!G.nkev) return;
+    cudaEventSynchronize(G.kev[3*G.nkev - 1]);
+    for(int i = 0; i < G.nkev; i++){
+        float x = 0, y = 0;
+        cudaEventElapsedTime(&x, G.kev[3*i], G.kev[3*i + 1]); cudaEventElapsedTime(&y, G.kev[3*i + 1], G.kev[3*i + 2]);
+        G.f64_ms += x; G.dd_ms += y; G.f64_n++;
+    }
+    G.nkev = 0;
+}
+/* the event triple of the next timed pass (NULL: timing off or no events) */
+static cudaEvent_t *ktime_slot(void){
+    if(!KTIME) return NULL;
+    const int cap = (int)(sizeof G.kev/sizeof G.kev[0])/3;
+    if(G.nkev == cap) ktime_collect();
+    if(G.nkev >= G.kevn){
+        for(int j = 0; j < 3; j++) if(cudaEventCreate(&G.kev[3*G.nkev + j]) != cudaSuccess) return NULL;
+        G.kevn = G.nkev + 1;
+    }
+    return &G.kev[3*G.nkev++];
+}
+
 extern "C" int sqb_dev_init(int device){
     if(G.on) return 0;
     int nd = 0; CKR(cudaGetDeviceCount(&nd));
@@ -103,7 +127,6 @@ extern "C" int sqb_dev_init(int device){
     { cudaMemPool_t pool; CKR(cudaDeviceGetDefaultMemPool(&pool, device));
       unsigned long long keep = ~0ULL; CKR(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)); }
     CKR(cudaEventCreate(&G.e0)); CKR(cudaEventCreate(&G.e1));
-    CKR(cudaEventCreate(&G.k0)); CKR(cudaEventCreate(&G.k1)); CKR(cudaEventCreate(&G.d1));
     CKR(cudaEventCreate(&G.t0)); CKR(cudaEventCreate(&G.t1));
     CKR(cudaMalloc(&G.acc, sizeof(sqb_acc_t)));
     CKR(cudaMalloc(&G.base, sizeof(unsigned long long)));
@@ -188,7 +211,8 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
         return 0;
     }
     CKR(cudaMemsetAsync(G.nfb, 0, sizeof(unsigned long long), G.s));
-    if(KTIME) CKR(cudaEventRecord(G.k0, G.s));
+    cudaEvent_t *ev = ktime_slot();
+    if(ev) CKR(cudaEventRecord(ev[0], G.s));
     if(use_split(g, a, t)){
         if(npts > G.ttcap){
             if(G.tt){ cudaFree(G.tt); cudaFree(G.ta); }
@@ -209,18 +233,13 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
         launch_f64(g, w, a, grid_for(g, w, npts, smem), smem, G.s);
         CKR(cudaGetLastError());
     }
-    if(KTIME) CKR(cudaEventRecord(G.k1, G.s));
+    if(ev) CKR(cudaEventRecord(ev[1], G.s));
     d.list = G.fb; d.nlist = G.nfb; d.listcap = G.cap; d.all = 0;
     /* the queue length is known only on the device: a persistent grid reads it */
     g->dd(&d, grid_for(g, 1, 1L << 30, smem), 128, smem, G.s);
     CKR(cudaGetLastError());
     G.launches += 2;
-    if(KTIME){
-        CKR(cudaEventRecord(G.d1, G.s));
-        CKR(cudaEventSynchronize(G.d1));
-        float x = 0, y = 0; cudaEventElapsedTime(&x, G.k0, G.k1); cudaEventElapsedTime(&y, G.k1, G.d1);
-        G.f64_ms += x; G.dd_ms += y; G.f64_n++;
-    }
+    if(ev) CKR(cudaEventRecord(ev[2], G.s));
     return 0;
 }
 
@@ -319,10 +338,12 @@ extern "C" int sqb_preload(const char *graph){
     return n;
 }
 /* instrumentation: kernels launched so far; with ktime on, the FP64 and double-double kernels of every
- * evaluation pass are bracketed by events (one synchronisation per batch) and their times summed */
+ * evaluation pass are bracketed by events, read when the host next waits on the stream, and their times
+ * summed */
 extern "C" unsigned long long sqb_launch_count(void){ return G.launches; }
 extern "C" void sqb_kernel_timing(int on){ KTIME = on; }
 extern "C" void sqb_kernel_times(double *f64_ms, double *dd_ms, long *f64_launches, int reset){
+    ktime_collect();
     *f64_ms = G.f64_ms; *dd_ms = G.dd_ms; *f64_launches = G.f64_n;
     if(reset){ G.f64_ms = G.dd_ms = 0; G.f64_n = 0; }
 }
@@ -538,6 +559,15 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
     long maxch = L->max_children > 0 ? L->max_children : (1L << 25);
     if(maxch < (1L << D)) maxch = 1L << D;
     long ncb = maxch >> D;
+    /* full batches hold whole rounds of tiles: the FP64 kernel's cap resident CTAs take tiles b, b + cap,
+     * ..., so with a multiple of cap tiles every CTA takes the same number and none idles while others
+     * finish one more */
+    {
+        int can0 = 0;
+        const long cap0 = grid_cap(g, f64_which(g, L->t.fma), 2*(2*G.K + 1)*sizeof(double), &can0);
+        const long round = (cap0*SQB_TILE) >> D;            /* cells per round (SQB_TILE >= 2^D) */
+        if(!L->t.alldd && can0 && round > 0 && ncb >= 2*round) ncb = (ncb/round)*round;
+    }
     if(reserve_points(ncb << D)) return -1;
     CKR(cudaMemsetAsync(G.acc, 0, sizeof(sqb_acc_t), G.s));
     CKR(cudaEventRecord(G.e0, G.s));
