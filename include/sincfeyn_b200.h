@@ -148,6 +148,22 @@ typedef int (*sqb_sym_eval_fn)(void *ctx, long n, const int *k, double *f, doubl
 int  sqb_sym_find(int D, sqb_sym_eval_fn fn, void *ctx, const char *spec, int *elems, char *desc, int ndesc,
                   double *worst, char *msg, int nmsg);
 
+/* The scaling test (`sincqed scale GRAPH [kappa] [seed]`, driver/main.c:76-115) with the raw
+ * double-double point function on the device: every direction e in {-E..E}^(n-1) \ {0} of the Schwinger
+ * parameters (E = SCALE_E, 1 by default) about random x0 (srand(seed)), |ptq(x) prod x| at kappa/3,
+ * 2 kappa/3 and kappa; a direction is slow if ratio = g(kappa)/g(2 kappa/3) > 0.3 and g(kappa) > 1e-30.
+ * Returns 0, 1 if the graph has no raw point function (VP graphs: the reference prints "no scale test"),
+ * or -1 (sqb_error()). */
+typedef struct {
+    int n, fixed;              /* Schwinger parameters, the fixed one */
+    long ndir;                 /* directions tested: (2E+1)^(n-1) - 1 */
+    int slow;                  /* slow directions */
+    double worst;              /* the largest ratio, its direction (index and exponents) and g there */
+    long worst_dir; int worst_e[16]; double worst_g[3];
+    int listed_e[12][16]; double listed_g[12][3];   /* the first min(slow, 12) slow directions */
+} sqb_scale_result_t;
+int  sqb_scale_test(const char *graph, double kappa, unsigned seed, int E, sqb_scale_result_t *r);
+
 /* the graphs compiled into this library: name, Volkov string, L, D, mirror weight */
 int  sqb_graph_count(void);
 const char *sqb_graph_name(int i);

@@ -190,6 +190,7 @@ def count_flops(graphs):
          '#define SQ_TABLE static const', '#define SQ_FUNC', '#define SQ_FUNC_K', '#define SQ_CHUNK', '#define SQ_CHUNK_DD', '#define RABS(x) sq_rabs(x)',
          '#define SQ_EXP(x) sq_exp(x)', '#define SQ_LOG(x) sq_log(x)', '#define SQG_NS(n) sqg_##n',
          '#define SQ_GRAPH_SPLIT(NAME, VOLKOV, L, D, W, NP, FIX, NPARTS) SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)',
+         '#define SQ_SCALE(NAME)',
          '#define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX) \\',
          'static void count_##NAME(void){ sq_count sf[D], ab; for(int d = 0; d < D; d++) sf[d] = sq_count(0.7 + 0.37*d); \\',
          '  sq_flops = 0; sq_trans = 0; sqg_##NAME::K<sq_count, 1>::f_##NAME(sf, &ab); long a1 = sq_flops, t1 = sq_trans; \\',
@@ -263,8 +264,11 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     if _newer(bat_o, [os.path.join(CSRC, 'batch.cpp')] + hdrs):
         jobs_list.append([CXX] + CXXFLAGS + ['-pthread', '-c', os.path.join(CSRC, 'batch.cpp'), '-o', bat_o])
     sym_o = os.path.join(OBJ, 'sym.o')
-    if _newer(sym_o, [os.path.join(CSRC, 'sym.cpp')] + hdrs):
+    if _newer(sym_o, [os.path.join(CSRC, 'sym.cpp'), os.path.join(CSRC, 'sqb_rand.h')] + hdrs):
         jobs_list.append([CXX] + CXXFLAGS + ['-c', os.path.join(CSRC, 'sym.cpp'), '-o', sym_o])
+    sc_o = os.path.join(OBJ, 'scale.o')
+    if _newer(sc_o, [os.path.join(CSRC, 'scale.cpp'), os.path.join(CSRC, 'sqb_rand.h')] + hdrs):
+        jobs_list.append([CXX] + CXXFLAGS + ['-c', os.path.join(CSRC, 'scale.cpp'), '-o', sc_o])
     n = jobs or min(len(jobs_list) or 1, os.cpu_count() or 4)
     if verbose and jobs_list:
         print('sincfeyn_b200: compiling %d objects with %d jobs' % (len(jobs_list), n), file=sys.stderr)
@@ -280,7 +284,7 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     with open(OCC, 'w') as f:
         json.dump(occ, f, indent=0, sort_keys=True)
     objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + \
-           [os.path.join(OBJ, 'kf_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o, bat_o, ck_o, sym_o]
+           [os.path.join(OBJ, 'kf_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o, bat_o, ck_o, sym_o, sc_o]
     if _newer(LIBSO, objs):
         _run([NVCC] + ARCH + ['-shared', '-o', LIBSO] + objs + ['-Xcompiler', '-fopenmp', '-lgomp', '-lpthread'])
     main_cpp = os.path.join(CSRC, 'main.cpp')

@@ -44,6 +44,10 @@ class KernelSource:
             raise ValueError('%s: no graph descriptor' % path)
         self.name, self.volkov = m.group(1), m.group(3)
         self.L, self.D, self.weight, self.n, self.fixed = (int(m.group(i)) for i in range(4, 9))
+        # the descriptor's remaining fields: fd, fq, ptd, ptq[, fv]; a graph with a raw QREAL point function
+        # (ptq) has the scaling test (driver/main.c:197; VP graphs have 0 there)
+        rest = txt[m.end():txt.index('}', m.end())].split(',')
+        self.has_ptq = len(rest) > 3 and rest[3].strip() == 'pt_%s_q' % self.name
         self.gl = []
         for g in _GL.finditer(txt):
             self.gl.append((g.group(1), int(g.group(2)), g.group(3)))
@@ -59,6 +63,8 @@ class KernelSource:
         self.funcs = [(m.group(1), m.group(2)) for m in _FDEF.finditer(self.qhalf)]
         if ('REAL', 'f_' + self.name) not in self.funcs:
             raise ValueError('%s: no f_%s in the QREAL half' % (path, self.name))
+        if self.has_ptq and ('REAL', 'pt_' + self.name) not in self.funcs:
+            raise ValueError('%s: the descriptor names pt_%s_q, the QREAL half has no pt_%s' % (path, self.name, self.name))
 
     def chunk(self, fname):
         return re.match(r'(bk|ab)_', fname) is not None
@@ -210,6 +216,8 @@ def emit(src):
     else:
         out.append('SQ_GRAPH(%s, "%s", %d, %d, %d, %d, %d)' % (k.name, k.volkov.replace('"', '\\"'),
                                                             k.L, k.D, k.weight, k.n, k.fixed))
+    if k.has_ptq:
+        out.append('SQ_SCALE(%s)' % k.name)
     return k, '\n'.join(out) + '\n'
 
 

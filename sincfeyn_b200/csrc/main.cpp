@@ -79,8 +79,35 @@ int main(int argc, char **argv){
         printf("%d graphs (one per mirror pair; w = mirror weight), precision fallback double-double on the GPU\n", NG);
         for(int i = 0; i < NG; i++){ int info[6]; const char *n = sqb_graph_name(i); sqb_graph_info(n, info);
             printf("  %-8s L=%d  %-22s D=%d w=%d\n", n, info[0], sqb_graph_volkov(n), info[1], info[2]); }
-        printf("usage: %s run h N [eps] [top] GRAPH...\n", argv[0]);
+        printf("usage: %s run h N [eps] [top] GRAPH... | scale GRAPH [kappa] [seed]\n", argv[0]);
         return 0;
+    }
+    /* the scaling test (driver/main.c:192-199), on the device */
+    if(!strcmp(argv[1], "scale")){
+        if(argc < 3) return 1;
+        const double kap = argc > 3 ? atof(argv[3]) : 24; const unsigned seed = argc > 4 ? atoi(argv[4]) : 1;
+        const int E = getenv("SCALE_E") ? atoi(getenv("SCALE_E")) : 1;
+        int rc = 0;
+        for(int i = 0; i < NG; i++){
+            int info[6]; const char *n = sqb_graph_name(i); sqb_graph_info(n, info);
+            const char *volkov = sqb_graph_volkov(n);
+            if(!selected(n, volkov, info[0], argv[2])) continue;
+            sqb_scale_result_t r;
+            const int k = sqb_scale_test(n, kap, seed, E, &r);
+            if(k == 1){ printf("%-6s %-22s (no scale test for VP graphs)\n", n, volkov); continue; }
+            if(k < 0){ fprintf(stderr, "sincqed: %s\n", sqb_error()); rc = 2; continue; }
+            for(int j = 0; j < r.slow && j < 12; j++){
+                printf("  slow direction e=(");
+                for(int q = 0; q < r.n; q++) if(q != r.fixed) printf("%+d", r.listed_e[j][q]);
+                printf(")  |g| at kappa/3,2/3,1: %.3e %.3e %.3e\n", r.listed_g[j][0], r.listed_g[j][1], r.listed_g[j][2]);
+            }
+            printf("%-6s %-22s scale test kappa=%g: %ld directions, %d slow (ratio>0.3), worst ratio %.3g (dir %ld: e=(",
+                   n, volkov, kap, r.ndir, r.slow, r.worst, r.worst_dir);
+            for(int q = 0; q < r.n; q++) if(q != r.fixed) printf("%+d", r.worst_e[q]);
+            printf(") |g| %.2e %.2e %.2e)\n", r.worst_g[0], r.worst_g[1], r.worst_g[2]);
+            fflush(stdout);
+        }
+        return rc;
     }
     if(strcmp(argv[1], "run")){ fprintf(stderr, "unknown command %s\n", argv[1]); return 1; }
     if(argc < 5){ fprintf(stderr, "run h N [eps] [top] GRAPH...\n"); return 1; }

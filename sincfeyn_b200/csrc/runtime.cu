@@ -364,7 +364,7 @@ __device__ int orbit_size(const sqb_sym_t &s, const int *k, int D){
     int stab = 1;
     for(int e = 1; e < s.n; e++){
         int c = 0;
-        for(int i = 0; i < D && !c; i++){ const int x = k[i], y = k[s.g[e][i]]; if(x != y) c = x < y ? -1 : 1; }
+        for(int i = 0; i < D && !c; i++){ const int x = k[i], y = k[(unsigned)s.g[e][i] % (unsigned)D]; if(x != y) c = x < y ? -1 : 1; }
         if(c > 0) return 0;
         if(!c) stab++;
     }
@@ -534,18 +534,19 @@ __global__ void __launch_bounds__(RT) sqb_k_scatter(const lvl_t a, const unsigne
         /* the child, then (under a fold) the other members of its orbit in group order, each once
          * (symorbit(), driver/sum.c:38-46), all with the child's flags (driver/sum.c:741-744) */
         const int ng = a.sym.n > 1 ? a.sym.n : 1;
+        const unsigned uD = (unsigned)a.D;
         for(int e = 0; e < ng; e++){
             bool dup = false;
             for(int f = 0; f < e && !dup; f++){
                 bool eq = true;
-                for(int d = 0; d < a.D && eq; d++) eq = k[a.sym.g[e][d]] == k[a.sym.g[f][d]];
+                for(int d = 0; d < a.D && eq; d++) eq = k[(unsigned)a.sym.g[e][d] % uD] == k[(unsigned)a.sym.g[f][d] % uD];
                 dup = eq;
             }
             if(dup) continue;
             if((long)o >= cap){ atomicAdd(overflow, 1ULL); o++; continue; }
             union { signed char k[SQB_MAXD]; int w[3]; } q;
             q.w[0] = q.w[1] = q.w[2] = 0;
-            for(int d = 0; d < a.D; d++) q.k[d] = (signed char)(e ? k[a.sym.g[e][d]] : k[d]);
+            for(int d = 0; d < a.D; d++) q.k[d] = (signed char)(e ? k[(unsigned)a.sym.g[e][d] % uD] : k[d]);
             q.k[SQB_PFLAG] = fl;
             int *dst = (int*)(next + o);
             dst[0] = q.w[0]; dst[1] = q.w[1]; dst[2] = q.w[2];
@@ -576,7 +577,12 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
         const sqb_pt_t *cells = L->cells + c0;
         sqb_eval_t a; memset(&a, 0, sizeof a); fill_eval(&a, &L->t);
         a.pts = cells; a.n = nc; a.esize = 1; a.stride = SQB_MAXD; a.flag_at = SQB_PFLAG; a.cells = 1; a.st = L->st;
-        if(L->sym && L->sym->n > 1) a.sym = *L->sym;
+        if(L->sym && L->sym->n > 1){
+            bool ok = L->sym->n <= SQB_SYMG;
+            for(int e = 0; ok && e < L->sym->n; e++) for(int i = 0; i < D; i++) ok = ok && L->sym->g[e][i] >= 0 && L->sym->g[e][i] < D;
+            if(!ok){ snprintf(g_err, sizeof g_err, "symmetry group: %d elements or an axis outside 0..%d", L->sym->n, D - 1); return -1; }
+            a.sym = *L->sym;
+        }
         /* level mode: the FP64 pass sums the tiles without fallback points (the all-dd form has no FP64
          * pass: the reduce kernel sums every tile) */
         int can = 0;
@@ -584,7 +590,8 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
         const bool fused = !L->t.alldd && can && !use_split(g, &a, &L->t) && nch >= 2*SQB_TILE*cap;
         if(fused){ a.part = G.bp; a.tkeep = G.bkeep; a.tfb = G.tfb; a.pw = L->pw; a.thr = L->thr; a.last = L->last; }
         if(eval_batch(g, &a, &L->t, nch)) return -1;
-        lvl_t r; r.cells = (const signed char*)cells; r.n = nch; r.D = D; r.st = L->st; r.last = L->last;
+        lvl_t r; memset(&r, 0, sizeof r);
+        r.cells = (const signed char*)cells; r.n = nch; r.D = D; r.st = L->st; r.last = L->last;
         r.abskip = L->t.abskip; r.pw = L->pw; r.thr = L->thr; r.v = G.v; r.uu = G.uu; r.stt = G.stt;
         r.sym = a.sym;
         const long nb = (nch + RTILE - 1)/RTILE;
@@ -785,6 +792,26 @@ extern "C" int sqb_eval_points_impl(const sqb_graph_t *g, long n, const double *
     return rc;
 }
 
+/* the scaling test's device part: a->g[3 ndir] for the directions of a, with the factor table xs
+ * (3 x (2E+1), host); the values come back to g_host.  Returns 0, 1 if the graph has no raw point
+ * function, or -1 */
+extern "C" int sqb_dev_scale(const sqb_graph_t *g, sqb_scale_t *a, const double *xs, double *g_host){
+    if(!g->scale) return 1;
+    const size_t nxs = 3*(size_t)(2*a->E + 1), ng = 3*(size_t)a->ndir;
+    double *blk = NULL;
+    CKR(cudaMallocAsync((void**)&blk, (nxs + ng)*sizeof(double), G.s));
+    a->xs = blk; a->g = blk + nxs;
+    CKR(cudaMemcpyAsync(blk, xs, nxs*sizeof(double), cudaMemcpyHostToDevice, G.s));
+    long want = ((long)ng + 127)/128, full = (long)G.nsm*4;
+    g->scale(a, (int)(want < full ? want : full), 128, G.s);
+    CKR(cudaGetLastError());
+    G.launches++;
+    CKR(cudaMemcpyAsync(g_host, a->g, ng*sizeof(double), cudaMemcpyDeviceToHost, G.s));
+    CKR(cudaStreamSynchronize(G.s));
+    cudaFreeAsync(blk, G.s);
+    return 0;
+}
+
 /* FP64 peak probe: independent chains of fused multiply-adds (8 per thread, unrolled) or of adds, on
  * every SM; flops = 2 per FMA, 1 per add.  The measured rate is the denominator of the evaluation
  * kernels' roofline (the device has no vendor FP64 figure in this environment). */
@@ -832,7 +859,8 @@ extern "C" int sqb_level_tail(const void *cells, long nchildren, int D, int st, 
                               const double *v, const double *uu, const unsigned char *stt,
                               void *bp, unsigned *bkeep, unsigned long long *boff, sqb_acc_t *acc, unsigned long long *base,
                               void *next, long next_cap, void *stream){
-    lvl_t r; r.cells = (const signed char*)cells; r.n = nchildren; r.D = D; r.st = st; r.last = last;
+    lvl_t r; memset(&r, 0, sizeof r);        /* no symmetry fold here (r.sym.n = 0) */
+    r.cells = (const signed char*)cells; r.n = nchildren; r.D = D; r.st = st; r.last = last;
     r.abskip = abskip; r.pw = pw; r.thr = thr; r.v = v; r.uu = uu; r.stt = stt;
     const long nb = (nchildren + RTILE - 1)/RTILE;
     cudaStream_t s = (cudaStream_t)stream;

@@ -80,6 +80,19 @@ typedef struct {
     double *uu;                   /* per point: e^2 of the round column (driver/eval.c:26) */
 } sqb_dd_t;
 
+/* The scaling test (sincqed scale, driver/main.c:79-115): for direction d (exponent e_i in -E..E of each
+ * Schwinger parameter but the fixed one, base-(2E+1) digits of d) and q = 0, 1, 2 the parameters
+ * x_i = x0_i * xs[q][e_i + E] (xs[q][j] = exp(-kappa (q+1)/3 (j - E)), double-double products),
+ * meas = prod_{i != fixed} x_i, and g[3 d + q] = |(double)(ptq(x, 0) meas)|; 0 for d = 0 */
+#define SQB_SCALE_MAXN 16
+typedef struct {
+    int n, fixed, E;
+    long ndir;
+    double x0[SQB_SCALE_MAXN];
+    const double *xs;             /* device: 3 x (2E+1) */
+    double *g;                    /* device: 3 ndir */
+} sqb_scale_t;
+
 typedef struct {
     int regs, local_bytes, max_threads, blocks_per_sm;
     int fused;                    /* FP64 kernel: sums level tiles itself (level mode available) */
@@ -104,6 +117,8 @@ typedef struct {
     void (*split)(int P, int fma, const sqb_eval_t *a, double *tt, double *ta, int grid, int block, size_t smem,
                   void *stream);
     int (*split_attr)(int P, int fma, int block, size_t smem, sqb_kattr_t *out);
+    /* the scaling test on the raw double-double point function ptq; NULL for graphs without one (VP) */
+    void (*scale)(const sqb_scale_t *a, int grid, int block, void *stream);
 } sqb_graph_t;
 
 #ifdef __cplusplus

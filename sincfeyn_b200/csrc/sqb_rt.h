@@ -76,6 +76,9 @@ void sqb_grow_end(void);
 const char *sqb_top_error(void);
 int  sqb_radix_sort_u64(unsigned long long *keys_dev, long n, int nbits, void *stream);
 
+/* the scaling test on the device (runtime.cu): 0, 1 = the graph has no raw point function, -1 */
+int  sqb_dev_scale(const sqb_graph_t *g, sqb_scale_t *a, const double *xs, double *g_host);
+
 /* instrumentation (runtime.cu, topgrid.cu) */
 unsigned long long sqb_launch_count(void);
 unsigned long long sqb_top_launches(void);

@@ -371,6 +371,29 @@ static int sqb_split_attr(int P, int block, size_t smem, sqb_kattr_t *o){
     return sqb_attr_of(sqb_k_fin<F, D>, block, smem, o);
 }
 
+/* the scaling test (sqb_scale_t): one thread per (direction, q); P::pt is the graph's raw double-double
+ * point function (pt_<name> of the QREAL half, SQ_AB = 1 as the reference's default) */
+template<class P>
+__global__ void __launch_bounds__(SQB_BLOCK) sqb_k_scale(const sqb_scale_t a){
+    const int B = 2*a.E + 1;
+    for(long j = blockIdx.x*(long)blockDim.x + threadIdx.x; j < 3*a.ndir; j += (long)gridDim.x*blockDim.x){
+        const long d = j/3; const int q = (int)(j - 3*d);
+        int e[SQB_SCALE_MAXN], nz = 0; long r = d;
+        for(int i = 0; i < a.n; i++){
+            if(i == a.fixed){ e[i] = 0; continue; }
+            e[i] = (int)(r % B) - a.E; r /= B; nz += e[i] != 0;
+        }
+        if(!nz){ a.g[j] = 0; continue; }
+        sqdd x[SQB_SCALE_MAXN], meas(1.0), ab;
+        for(int i = 0; i < a.n; i++){
+            x[i] = sqdd(a.x0[i])*sqdd(a.xs[q*B + e[i] + a.E]);
+            if(i != a.fixed) meas = meas*x[i];
+        }
+        const sqdd v = P::pt(x, sqdd(0.0), &ab);
+        a.g[j] = fabs((v*meas).value());
+    }
+}
+
 /* SQ_GRAPH(name, volkov, L, D, weight, n, fixed): the generated file ends with it, after namespace
  * SQG_NS(name) with the class template K<Real, SQ_AB> holding f_<name>.
  *
@@ -390,6 +413,7 @@ struct FS {                                                                     
 };                                                                                                 \
 }
 #if defined(SQB_FMA_TU)
+#define SQ_SCALE(NAME)
 #define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
 namespace SQG_NS(NAME) {                                                                           \
 struct F {                                                                                         \
@@ -415,8 +439,19 @@ extern "C" void SQB_##NAME##_splitfma(int P, const sqb_eval_t *a, double *tt, do
 extern "C" int SQB_##NAME##_splitattrfma(int P, int block, size_t smem, sqb_kattr_t *o){          \
     return sqb_split_attr<SQG_NS(NAME)::FS, D, NPARTS>(P, block, smem, o); }
 #else
+/* SQ_SCALE(name) follows SQ_GRAPH for a graph with a raw point function: its scaling-test launcher */
+#define SQ_SCALE(NAME)                                                                              \
+namespace SQG_NS(NAME) {                                                                           \
+struct PT {                                                                                        \
+    static __device__ __forceinline__ sqdd pt(const sqdd *x, sqdd Vx, sqdd *ab){                   \
+        return KD<sqdd, 1>::pt_##NAME(x, Vx, ab); }                                                \
+};                                                                                                 \
+}                                                                                                  \
+extern "C" void SQB_##NAME##_scale(const sqb_scale_t *a, int grid, int block, void *st){           \
+    sqb_k_scale<SQG_NS(NAME)::PT><<<grid, block, 0, (cudaStream_t)st>>>(*a); }
 #define SQ_GRAPH_CORE(NAME, D)                                                                      \
 extern "C" void SQB_##NAME##_f64fma(const sqb_eval_t *, int, int, size_t, void *) __attribute__((weak)); \
+extern "C" void SQB_##NAME##_scale(const sqb_scale_t *, int, int, void *) __attribute__((weak));   \
 extern "C" int SQB_##NAME##_attrfma(int, size_t, sqb_kattr_t *) __attribute__((weak));             \
 namespace SQG_NS(NAME) {                                                                           \
 struct F {                                                                                         \
@@ -444,7 +479,8 @@ static int attr(int which, int block, size_t smem, sqb_kattr_t *o){             
 #define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
 SQ_GRAPH_CORE(NAME, D)                                                                             \
 extern "C" const sqb_graph_t SQB_##NAME = {#NAME, VOLKOV, L, D, W, NP, FIX, 0,                     \
-    SQG_NS(NAME)::f64, SQG_NS(NAME)::dd, SQG_NS(NAME)::attr, SQB_##NAME##_f64fma, 0, NULL, NULL};
+    SQG_NS(NAME)::f64, SQG_NS(NAME)::dd, SQG_NS(NAME)::attr, SQB_##NAME##_f64fma, 0, NULL, NULL,     \
+    SQB_##NAME##_scale};
 #define SQ_GRAPH_SPLIT(NAME, VOLKOV, L, D, W, NP, FIX, NPARTS)                                      \
 SQ_GRAPH_CORE(NAME, D)                                                                             \
 SQ_SPLIT_F(NAME)                                                                                   \
@@ -462,5 +498,5 @@ static int split_attr(int P, int fma, int block, size_t smem, sqb_kattr_t *o){  
 }                                                                                                  \
 extern "C" const sqb_graph_t SQB_##NAME = {#NAME, VOLKOV, L, D, W, NP, FIX, 0,                     \
     SQG_NS(NAME)::f64, SQG_NS(NAME)::dd, SQG_NS(NAME)::attr, SQB_##NAME##_f64fma, NPARTS,           \
-    SQG_NS(NAME)::split, SQG_NS(NAME)::split_attr};
+    SQG_NS(NAME)::split, SQG_NS(NAME)::split_attr, SQB_##NAME##_scale};
 #endif

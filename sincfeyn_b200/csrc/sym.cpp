@@ -10,8 +10,7 @@
  * description and the worst deviation are the reference's.
  *
  * The random nodes come from the C library's rand() stream after srand(12345) and srand(4242)
- * (driver/sum.c:468, 528): glibc's rand() is random() on its default 128-byte state, which
- * initstate_r()/random_r() reproduce per call without touching the process-wide generator. */
+ * (driver/sum.c:468, 528), reproduced per call by sqb_rand.h. */
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -20,15 +19,12 @@
 #include <string>
 #include <vector>
 #include "sqb_rt.h"
+#include "sqb_rand.h"
 #include "sincfeyn_b200.h"
 
 namespace {
 
-struct Rng {
-    random_data rd; char st[128];
-    explicit Rng(unsigned seed){ memset(&rd, 0, sizeof rd); memset(st, 0, sizeof st); initstate_r(seed, st, sizeof st, &rd); }
-    int next(){ int32_t r = 0; random_r(&rd, &r); return (int)r; }
-};
+typedef SqbRand Rng;
 
 struct Finder {
     int D;

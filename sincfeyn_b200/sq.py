@@ -41,6 +41,13 @@ class Result(C.Structure):
                 ('sym_msg', C.c_char * 512)]
 
 
+class ScaleResult(C.Structure):
+    """sqb_scale_result_t: the scaling test of one graph (driver/main.c:76-115)."""
+    _fields_ = [('n', C.c_int), ('fixed', C.c_int), ('ndir', C.c_long), ('slow', C.c_int), ('worst', C.c_double),
+                ('worst_dir', C.c_long), ('worst_e', C.c_int * 16), ('worst_g', C.c_double * 3),
+                ('listed_e', (C.c_int * 16) * 12), ('listed_g', (C.c_double * 3) * 12)]
+
+
 class Job(C.Structure):
     """sqb_job_t: one integral of a batch."""
     _fields_ = [('graph', C.c_char_p), ('h', C.c_double), ('N', C.c_int), ('eps', C.c_double), ('top', C.c_int),
@@ -319,6 +326,24 @@ def sym_find(D, evaluate, spec='auto'):
         raise SqbError('symmetry search failed: %r' % (err[0] if err else 'evaluator'))
     elems = np.array(el[:], dtype=np.int64).reshape(64, 12)[:n, :D]
     return dict(order=n, elems=elems, desc=desc.value.decode(), worst=worst.value, msg=msg.value.decode())
+
+
+def scale_test(graph, kappa=24.0, seed=1, E=1):
+    """`sincqed scale GRAPH kappa seed` for one graph on the device: None for a graph without a raw point
+    function (VP), else a dict with the directions tested, the slow ones (first twelve listed with |g| at
+    kappa/3, 2kappa/3, kappa) and the worst ratio with its direction."""
+    L = lib()
+    L.sqb_scale_test.argtypes = [C.c_char_p, C.c_double, C.c_uint, C.c_int, C.POINTER(ScaleResult)]
+    r = ScaleResult()
+    rc = L.sqb_scale_test(graph.encode(), float(kappa), int(seed), int(E), C.byref(r))
+    if rc == 1:
+        return None
+    if rc:
+        raise SqbError('%s: %s' % (graph, L.sqb_error().decode()))
+    free = [i for i in range(r.n) if i != r.fixed]
+    return dict(n=r.n, fixed=r.fixed, ndir=r.ndir, slow=r.slow, worst=r.worst, worst_dir=r.worst_dir,
+                worst_e=[r.worst_e[i] for i in free], worst_g=list(r.worst_g),
+                listed=[([r.listed_e[j][i] for i in free], list(r.listed_g[j])) for j in range(min(r.slow, 12))])
 
 
 def eval_points(graph, sf, prec=0, ab=1):

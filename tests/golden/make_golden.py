@@ -21,13 +21,16 @@ Fixtures
   synth_runs.json               the reference's hsum() on the synthetic integrands, -ffp-contract=off build,
                                 SINCQED_SYM=0 and SINCQED_KEEPBT=1 (one boundary table, the exact grow):
                                 syn_d5 at h = 1.0 (N = 61) and h = 0.7 (N = 87), syn_d8 at h = 1.0 (N = 61)
+  scale.json                    `sincqed scale SEL kappa seed` of the -ffp-contract=off build, one thread
+                                (directions in order): the stdout lines per graph, kappa = 24 for all2, g3_00,
+                                g3_07, g3_lbl, v3_00 and kappa = 3 (slow directions listed) for g2_00, g3_07
   fold.json                     the symmetry fold (driver/sum.c:21-46, 464-592), -ffp-contract=off build:
                                 the group line the reference prints for every graph of g2 g3 v3 v4 w4
                                 (`run 2.0 13 1e-4 GRAPH`, SINCQED_SYM unset = auto; the search's nodes only
                                 need K >= 6), and folded sums (SINCQED_SYM unset, SINCQED_KEEPBT=1) with
                                 top = 2 so that kept orbits go on to a second refinement level
 
-    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold]   # default: all of them
+    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold scale]   # default: all of them
 """
 import json
 import os
@@ -120,6 +123,29 @@ _SYMLINE = re.compile(r'^# (\S+): symmetry fold sigma=(.*) \(group of order (\d+
                       r'max \|f\(k\)-f\(k sigma\)\|/sum\|terms\| over 200 nodes (\S+)$', re.M)
 
 
+SCALE_RUNS = [('all2', 24, 1), ('g3_00', 24, 1), ('g3_07', 24, 1), ('g3_lbl', 24, 1), ('v3_00', 24, 1),
+              ('g2_00', 3, 2), ('g3_07', 3, 5)]      # kappa = 3: slow directions (ratio ~ e^-1) to list
+
+
+def scale():
+    d = {'E': 1, 'runs': []}
+    env = dict(os.environ, OMP_NUM_THREADS='1', SINCQED_LOG='-', SINCQED_RESULTS='-')
+    env.pop('SCALE_E', None)
+    for sel, kappa, seed in SCALE_RUNS:
+        out = subprocess.run([refpy.SINCQED_EXACT, 'scale', sel, str(kappa), str(seed)], env=env,
+                             stdout=subprocess.PIPE, text=True, check=True, timeout=3600).stdout
+        run, cur = {'sel': sel, 'kappa': kappa, 'seed': seed, 'lines': {}}, []
+        for line in out.splitlines():
+            if line.startswith('  slow direction'):
+                cur.append(line)
+            elif 'scale test kappa=' in line or '(no scale test' in line:
+                run['lines'][line.split()[0]] = cur + [line]
+                cur = []
+        d['runs'].append(run)
+    with open(os.path.join(OUT, 'scale.json'), 'w') as f:
+        json.dump(d, f, indent=1)
+
+
 def fold():
     h, N, eps = FOLD_GROUP_RUN
     d = {'group_run': {'h': h, 'N': N, 'eps': eps}, 'groups': {}, 'runs': [], 'env': {'SINCQED_KEEPBT': '1'}}
@@ -139,7 +165,7 @@ def fold():
 
 
 if __name__ == '__main__':
-    parts = sys.argv[1:] or ['all2', 'boxsum', 'pointwise', 'synth', 'fold']
+    parts = sys.argv[1:] or ['all2', 'boxsum', 'pointwise', 'synth', 'fold', 'scale']
     if 'all2' in parts:
         all2()
     if 'boxsum' in parts:
@@ -154,3 +180,5 @@ if __name__ == '__main__':
         synth()
     if 'fold' in parts:
         fold()
+    if 'scale' in parts:
+        scale()

@@ -34,6 +34,7 @@ SRC = r'''
 #define SQ_LOG(x) sq_log(x)
 #define SQG_NS(n) sqg_##n
 #define SQ_GRAPH_SPLIT(NAME, VOLKOV, L, D, W, NP, FIX, NPARTS) SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)
+#define SQ_SCALE(NAME)
 #define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
 extern "C" int hg_##NAME(long n, const double *sf, int prec, int ab, double *f, double *a){       \
     for(long i = 0; i < n; i++){                                                                   \
