@@ -163,6 +163,11 @@ typedef struct {
     int listed_e[12][16]; double listed_g[12][3];   /* the first min(slow, 12) slow directions */
 } sqb_scale_result_t;
 int  sqb_scale_test(const char *graph, double kappa, unsigned seed, int E, sqb_scale_result_t *r);
+/* its host halves, for a caller that evaluates the point function itself: the base point x0[n] and the
+ * factor table xs[3 (2E+1)] (xs[q (2E+1) + e + E] = exp(-kappa (q+1)/3 e)); and the summary of the values
+ * g[3 d + q] over the (2E+1)^(n-1) directions d */
+void sqb_scale_setup(int n, int fixed, double kappa, unsigned seed, int E, double *x0, double *xs);
+void sqb_scale_summary(int n, int fixed, int E, long ndir, const double *g, sqb_scale_result_t *r);
 
 /* the graphs compiled into this library: name, Volkov string, L, D, mirror weight */
 int  sqb_graph_count(void);

@@ -20,6 +20,38 @@
 
 extern "C" void sqb_set_error_msg(const char *msg);
 
+/* the host half: the random base point and factor table of driver/main.c:80-96 */
+extern "C" void sqb_scale_setup(int n, int fixed, double kappa, unsigned seed, int E, double *x0, double *xs){
+    SqbRand rng(seed);
+    for(int i = 0; i < n; i++) x0[i] = exp(4.0*rng.next()/RAND_MAX - 2.0);
+    x0[fixed] = 1;
+    const int B = 2*E + 1;
+    for(int q = 0; q < 3; q++){
+        const double kk = kappa*(q + 1)/3.0;
+        for(int e = -E; e <= E; e++) xs[q*B + e + E] = exp(-kk*e);
+    }
+}
+/* ... and the directions in order over the values g[3 d + q] (driver/main.c:98-108, one thread) */
+extern "C" void sqb_scale_summary(int n, int fixed, int E, long ndir, const double *gv, sqb_scale_result_t *r){
+    const int B = 2*E + 1;
+    r->n = n; r->fixed = fixed; r->ndir = ndir - 1; r->slow = 0; r->worst = 0; r->worst_dir = -1;
+    for(long d = 0; d < ndir; d++){
+        int e[SQB_SCALE_MAXN] = {0}, nz = 0; long q = d;
+        for(int i = 0; i < n; i++){ if(i == fixed){ e[i] = 0; continue; } e[i] = (int)(q % B) - E; q /= B; nz += e[i] != 0; }
+        if(!nz) continue;
+        const double *gd = &gv[3*d];
+        const double ratio = gd[1] > 0 ? gd[2]/gd[1] : 0;
+        if(ratio > r->worst){
+            r->worst = ratio; r->worst_dir = d;
+            memcpy(r->worst_g, gd, sizeof r->worst_g); memcpy(r->worst_e, e, sizeof e);
+        }
+        if(ratio > 0.3 && gd[2] > 1e-30){
+            if(r->slow < 12){ memcpy(r->listed_e[r->slow], e, sizeof e); memcpy(r->listed_g[r->slow], gd, sizeof r->listed_g[0]); }
+            r->slow++;
+        }
+    }
+}
+
 extern "C" int sqb_scale_test(const char *graph, double kappa, unsigned seed, int E, sqb_scale_result_t *r){
     char msg[256];
     memset(r, 0, sizeof *r);
@@ -41,31 +73,10 @@ extern "C" int sqb_scale_test(const char *graph, double kappa, unsigned seed, in
     if(sqb_dev_init(0)){ snprintf(msg, sizeof msg, "device: %s", sqb_last_error()); sqb_set_error_msg(msg); return -1; }
     sqb_scale_t a; memset(&a, 0, sizeof a);
     a.n = n; a.fixed = fixed; a.E = E; a.ndir = ndir;
-    SqbRand rng(seed);
-    for(int i = 0; i < n; i++) a.x0[i] = exp(4.0*rng.next()/RAND_MAX - 2.0);
-    a.x0[fixed] = 1;
     std::vector<double> xs(3*(size_t)B), gv(3*(size_t)ndir);
-    for(int q = 0; q < 3; q++){
-        const double kk = kappa*(q + 1)/3.0;
-        for(int e = -E; e <= E; e++) xs[q*B + e + E] = exp(-kk*e);
-    }
+    sqb_scale_setup(n, fixed, kappa, seed, E, a.x0, xs.data());
     const int rc = sqb_dev_scale(g, &a, xs.data(), gv.data());
     if(rc < 0){ snprintf(msg, sizeof msg, "device: %s", sqb_last_error()); sqb_set_error_msg(msg); return -1; }
-    r->ndir = ndir - 1;
-    for(long d = 0; d < ndir; d++){
-        int e[SQB_SCALE_MAXN] = {0}, nz = 0; long q = d;
-        for(int i = 0; i < n; i++){ if(i == fixed){ e[i] = 0; continue; } e[i] = (int)(q % B) - E; q /= B; nz += e[i] != 0; }
-        if(!nz) continue;
-        const double *gd = &gv[3*d];
-        const double ratio = gd[1] > 0 ? gd[2]/gd[1] : 0;
-        if(ratio > r->worst){
-            r->worst = ratio; r->worst_dir = d;
-            memcpy(r->worst_g, gd, sizeof r->worst_g); memcpy(r->worst_e, e, sizeof e);
-        }
-        if(ratio > 0.3 && gd[2] > 1e-30){
-            if(r->slow < 12){ memcpy(r->listed_e[r->slow], e, sizeof e); memcpy(r->listed_g[r->slow], gd, sizeof r->listed_g[0]); }
-            r->slow++;
-        }
-    }
+    sqb_scale_summary(n, fixed, E, ndir, gv.data(), r);
     return 0;
 }

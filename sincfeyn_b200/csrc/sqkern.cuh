@@ -19,6 +19,7 @@
 #include <math.h>
 #include "sqdd.cuh"
 #include "sqb_internal.h"
+#include "sqscale.cuh"
 
 #ifndef SQG_NS
 #define SQG_NS(n) sqg_##n                    /* the graph's namespace (sqgf_<name> in the contracted unit) */
@@ -375,23 +376,8 @@ static int sqb_split_attr(int P, int block, size_t smem, sqb_kattr_t *o){
  * point function (pt_<name> of the QREAL half, SQ_AB = 1 as the reference's default) */
 template<class P>
 __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_scale(const sqb_scale_t a){
-    const int B = 2*a.E + 1;
-    for(long j = blockIdx.x*(long)blockDim.x + threadIdx.x; j < 3*a.ndir; j += (long)gridDim.x*blockDim.x){
-        const long d = j/3; const int q = (int)(j - 3*d);
-        int e[SQB_SCALE_MAXN], nz = 0; long r = d;
-        for(int i = 0; i < a.n; i++){
-            if(i == a.fixed){ e[i] = 0; continue; }
-            e[i] = (int)(r % B) - a.E; r /= B; nz += e[i] != 0;
-        }
-        if(!nz){ a.g[j] = 0; continue; }
-        sqdd x[SQB_SCALE_MAXN], meas(1.0), ab;
-        for(int i = 0; i < a.n; i++){
-            x[i] = sqdd(a.x0[i])*sqdd(a.xs[q*B + e[i] + a.E]);
-            if(i != a.fixed) meas = meas*x[i];
-        }
-        const sqdd v = P::pt(x, sqdd(0.0), &ab);
-        a.g[j] = fabs((v*meas).value());
-    }
+    for(long j = blockIdx.x*(long)blockDim.x + threadIdx.x; j < 3*a.ndir; j += (long)gridDim.x*blockDim.x)
+        a.g[j] = sqb_scale_value<P>(a, j);
 }
 
 /* SQ_GRAPH(name, volkov, L, D, weight, n, fixed): the generated file ends with it, after namespace

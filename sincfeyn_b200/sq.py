@@ -340,10 +340,36 @@ def scale_test(graph, kappa=24.0, seed=1, E=1):
         return None
     if rc:
         raise SqbError('%s: %s' % (graph, L.sqb_error().decode()))
+    return _scale_dict(r)
+
+
+def _scale_dict(r):
     free = [i for i in range(r.n) if i != r.fixed]
     return dict(n=r.n, fixed=r.fixed, ndir=r.ndir, slow=r.slow, worst=r.worst, worst_dir=r.worst_dir,
                 worst_e=[r.worst_e[i] for i in free], worst_g=list(r.worst_g),
                 listed=[([r.listed_e[j][i] for i in free], list(r.listed_g[j])) for j in range(min(r.slow, 12))])
+
+
+def scale_setup(n, fixed, kappa=24.0, seed=1, E=1):
+    """The scaling test's host half (sqb_scale_setup): the base point x0[n] and the factor table
+    xs[3, 2E+1] for a caller that evaluates the point function itself."""
+    L = lib()
+    L.sqb_scale_setup.argtypes = [C.c_int, C.c_int, C.c_double, C.c_uint, C.c_int, C.c_void_p, C.c_void_p]
+    x0 = np.zeros(n)
+    xs = np.zeros(3 * (2 * E + 1))
+    L.sqb_scale_setup(int(n), int(fixed), float(kappa), int(seed), int(E), x0.ctypes.data, xs.ctypes.data)
+    return x0, xs
+
+
+def scale_summary(n, fixed, E, g):
+    """The scaling test's summary (sqb_scale_summary) of values g[3 d + q] over the (2E+1)^(n-1)
+    directions, as scale_test() returns it."""
+    L = lib()
+    L.sqb_scale_summary.argtypes = [C.c_int, C.c_int, C.c_int, C.c_long, C.c_void_p, C.POINTER(ScaleResult)]
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    r = ScaleResult()
+    L.sqb_scale_summary(int(n), int(fixed), int(E), g.size // 3, g.ctypes.data, C.byref(r))
+    return _scale_dict(r)
 
 
 def eval_points(graph, sf, prec=0, ab=1):

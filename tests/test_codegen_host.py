@@ -24,6 +24,7 @@ NOT_BITWISE = {'g3_lbl': 'pt4_g3_lbl (double half) and pt_g3_lbl (QREAL half) ar
 SRC = r'''
 #include <math.h>
 #include "sqdd.cuh"
+#include "sqscale.cuh"
 #define SQ_TABLE static const
 #define SQ_FUNC
 #define SQ_FUNC_K
@@ -34,7 +35,11 @@ SRC = r'''
 #define SQ_LOG(x) sq_log(x)
 #define SQG_NS(n) sqg_##n
 #define SQ_GRAPH_SPLIT(NAME, VOLKOV, L, D, W, NP, FIX, NPARTS) SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)
-#define SQ_SCALE(NAME)
+#define SQ_SCALE(NAME)                                                                              \
+namespace sqg_##NAME { struct PT { static sqdd pt(const sqdd *x, sqdd Vx, sqdd *ab){                 \
+    return KD<sqdd, 1>::pt_##NAME(x, Vx, ab); } }; }                                                \
+extern "C" void hs_##NAME(const sqb_scale_t *a){                                                   \
+    for(long j = 0; j < 3*a->ndir; j++) a->g[j] = sqb_scale_value<sqg_##NAME::PT>(*a, j); }
 #define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
 extern "C" int hg_##NAME(long n, const double *sf, int prec, int ab, double *f, double *a){       \
     for(long i = 0; i < n; i++){                                                                   \
@@ -52,23 +57,31 @@ def hostlib(names):
     tag = '%d_%s' % (len(names), names[0])
     so = os.path.join(OUT, 'hostgen_%s.so' % tag)
     cuhs = [os.path.join(GEN, n + '.cuh') for n in names]
-    if not os.path.exists(so) or any(os.path.getmtime(c) > os.path.getmtime(so) for c in cuhs + [os.path.join(CSRC, 'sqdd.cuh')]):
-        cc = os.path.join(OUT, 'hostgen_%s.cc' % tag)
+    cc = os.path.join(OUT, 'hostgen_%s.cc' % tag)
+    text = SRC + ''.join('#include "%s"\n' % c for c in cuhs)
+    deps = cuhs + [os.path.join(CSRC, f) for f in ('sqdd.cuh', 'sqscale.cuh', 'sqb_internal.h')]
+    if not os.path.exists(so) or not os.path.exists(cc) or open(cc).read() != text or \
+            any(os.path.getmtime(c) > os.path.getmtime(so) for c in deps):
         with open(cc, 'w') as f:
-            f.write(SRC + ''.join('#include "%s"\n' % c for c in cuhs))
+            f.write(text)
         subprocess.run(['g++', '-O0', '-ffp-contract=off', '-std=c++17', '-shared', '-fPIC', '-I' + CSRC,
                         '-o', so, cc], check=True)
     return C.CDLL(so)
 
 
-@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3', 'v4', 'w4'])
-def test_generated_kernels_match_the_reference_bitwise(cls):
+def class_lib(cls):
+    """the host build of a class's generated kernels (those of the class's pointwise fixture)"""
     z = np.load(os.path.join(GOLD, 'pointwise_%s.npz' % cls))
     names = sorted({k.split('.')[0] for k in z.files})
     have = [n for n in names if os.path.exists(os.path.join(GEN, n + '.cuh'))]
     if not have:
         pytest.skip('no generated kernels for %s (python -m sincfeyn_b200.build)' % cls)
-    L = hostlib(have)
+    return z, have, hostlib(have)
+
+
+@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3', 'v4', 'w4'])
+def test_generated_kernels_match_the_reference_bitwise(cls):
+    z, have, L = class_lib(cls)
     for n in have:
         sf = np.ascontiguousarray(z[n + '.sf'])
         m = sf.shape[0]
@@ -91,3 +104,44 @@ def test_generated_kernels_match_the_reference_bitwise(cls):
         fn(m, sf.ctypes.data, 1, 1, f.ctypes.data, a.ctypes.data)
         want = z[n + '.fq']
         assert np.array_equal(np.concatenate([f, a], 1), want, equal_nan=True), (n, 'dd')
+
+
+class ScaleArgs(C.Structure):
+    """sqb_scale_t"""
+    _fields_ = [('n', C.c_int), ('fixed', C.c_int), ('E', C.c_int), ('ndir', C.c_long), ('x0', C.c_double * 16),
+                ('xs', C.c_void_p), ('g', C.c_void_p)]
+
+
+def test_scaling_test_values_match_the_reference():
+    """`sincqed scale` on the host build: the values of sqscale.cuh (the function the device kernel runs per
+    value) over the generated raw double-double point functions, with the library's host halves
+    (sqb_scale_setup, sqb_scale_summary), print every line of the reference's output
+    (tests/golden/scale.json); graphs without a raw point function (VP) have no scale entry"""
+    import json
+    from sincfeyn_b200 import sq
+    from scalefmt import scale_lines
+    with open(os.path.join(GOLD, 'scale.json')) as f:
+        gold = json.load(f)
+    libs = {cls: class_lib(cls)[2] for cls in ('g2', 'g3', 'v3')}
+    info = {g['name']: g for g in sq.graphs()}
+    E = gold['E']
+    checked = 0
+    for run in gold['runs']:
+        for name, want in run['lines'].items():
+            L = libs['g3' if name.startswith('g3_') else 'v3' if name.startswith('v3_') else 'g2']
+            if '(no scale test' in want[-1]:
+                assert not hasattr(L, 'hs_' + name), name
+                assert scale_lines(name, info[name]['volkov'], None, run['kappa']) == want
+                continue
+            n, fixed = info[name]['n'], info[name]['fixed']
+            ndir = (2 * E + 1) ** (n - 1)
+            x0, xs = sq.scale_setup(n, fixed, run['kappa'], run['seed'], E)
+            g = np.zeros(3 * ndir)
+            a = ScaleArgs(n, fixed, E, ndir)
+            a.x0[:n] = list(x0)
+            a.xs, a.g = xs.ctypes.data, g.ctypes.data
+            getattr(L, 'hs_' + name)(C.byref(a))
+            r = sq.scale_summary(n, fixed, E, g)
+            assert scale_lines(name, info[name]['volkov'], r, run['kappa']) == want, name
+            checked += 1
+    assert checked >= 8

@@ -15,6 +15,8 @@ import pytest
 
 from sincfeyn_b200 import sq
 
+from scalefmt import scale_lines as lines
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLD = os.path.join(ROOT, 'tests', 'golden', 'scale.json')
 CLI = os.path.join(ROOT, 'sincfeyn_b200', 'bin', 'sincqed')
@@ -22,18 +24,6 @@ pytestmark = pytest.mark.gpu
 
 with open(GOLD) as _f:
     SCALE = json.load(_f)
-
-
-def lines(name, volkov, r, kappa):
-    """the reference's printf lines (driver/main.c:104-113) from a result"""
-    if r is None:
-        return ['%-6s %-22s (no scale test for VP graphs)' % (name, volkov)]
-    out = ['  slow direction e=(%s)  |g| at kappa/3,2/3,1: %.3e %.3e %.3e' % (''.join('%+d' % x for x in e), *g)
-           for e, g in r['listed']]
-    out.append('%-6s %-22s scale test kappa=%g: %d directions, %d slow (ratio>0.3), worst ratio %.3g (dir %d: e=(%s) '
-               '|g| %.2e %.2e %.2e)' % (name, volkov, kappa, r['ndir'], r['slow'], r['worst'], r['worst_dir'],
-                                        ''.join('%+d' % x for x in r['worst_e']), *r['worst_g']))
-    return out
 
 
 CASES = [(r, name) for r in SCALE['runs'] for name in sorted(r['lines'])]
