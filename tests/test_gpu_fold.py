@@ -8,7 +8,9 @@ tests/golden/fold.json), with top = 2 so that kept orbits go on to a second refi
     loops) relative;
   - the fold leaves the kept tree alone: folded and unfolded device runs keep the same top level, agree
     within the same tolerance, and the folded one evaluates fewer points;
-  - the contracted kernels (the default) agree too, their evaluation counts within 1e-4."""
+  - the contracted kernels (the default) agree too, their evaluation counts within 1e-4;
+  - checkpoints: a folded run stopped after its first level and resumed is bit for bit the unbroken one,
+    and the reference (fold on) resumes the evaluator's folded checkpoint to its own folded result."""
 import json
 import os
 
@@ -54,3 +56,38 @@ def test_manual_group_and_refusals_on_the_device():
     b = sq.run(h, N, 1e-12, ['g3_07'], top=top, fma=0, sym='1,0,2,3,4')[0]
     assert b['raw']['sym_order'] == 1 and 'NOT SYMMETRIC' in b['raw']['sym_msg']
     assert b['evals'] > a['evals']
+
+
+EXACT = ('S', 'Ah', 'ref', 'prune', 'trunc', 'unres', 'nev', 'nq', 'kept_top', 'es1', 'es2', 'abskipped')
+
+
+def test_folded_stop_and_resume_is_bitwise(tmp_path):
+    """a folded run stopped after its first checkpoint (the kept orbits of the step-2h level, in list
+    order) and resumed gives every result field of the unbroken folded run"""
+    case = next(r for r in FOLD['runs'] if r['name'] == 'g3_07')
+    name, h, N, top = case['name'], case['h'], case['N'], case['top']
+    full = sq.hsum(name, h, N, 1e-12, top, sym='auto')
+    d = str(tmp_path)
+    assert sq.hsum(name, h, N, 1e-12, top, sym='auto', ckpt_every=600, ckpt_dir=d, ckpt_stop=1) is None
+    res = sq.hsum(name, h, N, 1e-12, top, sym='auto', ckpt_every=600, ckpt_dir=d)
+    for f in EXACT:
+        assert res[f] == full[f], (f, res[f], full[f])
+
+
+def test_reference_resumes_our_folded_checkpoint(tmp_path):
+    """the reference CPU build (fold on) resumes the evaluator's folded checkpoint and finishes with its
+    own folded run's evaluation count and value"""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'oracle'))
+    import refpy
+    if not refpy.available(refpy.SINCQED_EXACT):
+        pytest.skip('oracle/_ref not built')
+    case = next(r for r in FOLD['runs'] if r['name'] == 'g3_25')
+    name, h, N, top = case['name'], case['h'], case['N'], case['top']
+    d = str(tmp_path)
+    assert sq.hsum(name, h, N, 1e-12, top, fma=0, sym='auto', ckpt_every=600, ckpt_dir=d, ckpt_stop=1) is None
+    rows, out = refpy.run(refpy.SINCQED_EXACT, h, N, 1e-12, [name], top=top,
+                          env=dict(FOLD['env'], SINCQED_CKPT='600', SINCQED_CKPT_DIR=d))
+    assert 'resuming %s from checkpoint' % name in out
+    assert rows[0]['evals'] == case['evals'], (rows[0]['evals'], case['evals'])
+    assert abs(rows[0]['value'] - case['value']) <= 1e-11*abs(case['value'])
