@@ -84,6 +84,9 @@ typedef struct {
                               refinement levels evaluate only the children that are the minimum of their orbit,
                               weight each by the orbit size and keep whole orbits: the kept tree is unchanged, the
                               sums agree to rounding, and the evaluations drop by up to the group's order */
+    double predict;        /* SINCQED_PREDICT = alpha (0 = off, the default): at the last level a child whose mean
+                              |f| over the corners of its 2h cube (values of the level before, driver/sum.c:64-69)
+                              is below alpha*thr is not evaluated; a controlled extra pruning loss */
 } sqb_opts_t;
 #define SQB_CKPT_STOPPED 2 /* sqb_hsum's return code under ckpt_stop */
 
@@ -112,6 +115,7 @@ typedef struct {
     char sym_desc[256];
     double sym_worst;
     char sym_msg[512];
+    long pskip;            /* final-level points the predictor left out (PSKIP, driver/sum.c:806) */
 } sqb_result_t;
 
 void sqb_default_opts(sqb_opts_t *o);
@@ -168,6 +172,11 @@ int  sqb_scale_test(const char *graph, double kappa, unsigned seed, int E, sqb_s
  * g[3 d + q] over the (2E+1)^(n-1) directions d */
 void sqb_scale_setup(int n, int fixed, double kappa, unsigned seed, int E, double *x0, double *xs);
 void sqb_scale_summary(int n, int fixed, int E, long ndir, const double *g, sqb_scale_result_t *r);
+
+/* sizeof of a structure of this interface by its name ("sqb_opts_t", "sqb_result_t", "sqb_job_t",
+ * "sqb_ckpt_t", "sqb_scale_result_t"; and the internal level interface "sqb_level_t", "sqb_acc_t",
+ * "sqb_test_t", "sqb_scale_t"), so that a binding can check its copies; -1 if unknown */
+long sqb_struct_size(const char *name);
 
 /* the graphs compiled into this library: name, Volkov string, L, D, mirror weight */
 int  sqb_graph_count(void);

@@ -248,6 +248,9 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     tg_o = os.path.join(OBJ, 'topgrid.o')
     if _newer(tg_o, [os.path.join(CSRC, 'topgrid.cu')] + hdrs):
         jobs_list.append([NVCC] + NVFLAGS + ['-c', os.path.join(CSRC, 'topgrid.cu'), '-o', tg_o])
+    pr_o = os.path.join(OBJ, 'predict.o')
+    if _newer(pr_o, [os.path.join(CSRC, 'predict.cu')] + hdrs):
+        jobs_list.append([NVCC] + NVFLAGS + ['-c', os.path.join(CSRC, 'predict.cu'), '-o', pr_o])
     na_o = os.path.join(OBJ, 'noalloc.o')
     if _newer(na_o, [os.path.join(CSRC, 'noalloc.cu')] + hdrs):
         jobs_list.append([NVCC] + NVFLAGS + ['-c', os.path.join(CSRC, 'noalloc.cu'), '-o', na_o])
@@ -284,7 +287,7 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     with open(OCC, 'w') as f:
         json.dump(occ, f, indent=0, sort_keys=True)
     objs = [os.path.join(OBJ, 'k_%s.o' % g[0]) for g in graphs] + \
-           [os.path.join(OBJ, 'kf_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, na_o, reg_o, eng_o, bat_o, ck_o, sym_o, sc_o]
+           [os.path.join(OBJ, 'kf_%s.o' % g[0]) for g in graphs] + [rt_o, tg_o, pr_o, na_o, reg_o, eng_o, bat_o, ck_o, sym_o, sc_o]
     if _newer(LIBSO, objs):
         _run([NVCC] + ARCH + ['-shared', '-o', LIBSO] + objs + ['-Xcompiler', '-fopenmp', '-lgomp', '-lpthread'])
     main_cpp = os.path.join(CSRC, 'main.cpp')

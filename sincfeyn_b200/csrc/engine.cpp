@@ -51,6 +51,18 @@ extern "C" void sqb_default_opts(sqb_opts_t *o){
     o->fma = 1; o->split = 0;
 }
 
+/* sizeof of the structures a binding mirrors (the public ones and the level interface), so that a
+ * binding can check its copies; -1 for an unknown name */
+extern "C" long sqb_struct_size(const char *name){
+    static const struct { const char *n; long s; } T[] = {
+        {"sqb_opts_t", sizeof(sqb_opts_t)}, {"sqb_result_t", sizeof(sqb_result_t)}, {"sqb_job_t", sizeof(sqb_job_t)},
+        {"sqb_ckpt_t", sizeof(sqb_ckpt_t)}, {"sqb_scale_result_t", sizeof(sqb_scale_result_t)},
+        {"sqb_level_t", sizeof(sqb_level_t)}, {"sqb_acc_t", sizeof(sqb_acc_t)}, {"sqb_test_t", sizeof(sqb_test_t)},
+        {"sqb_scale_t", sizeof(sqb_scale_t)}};
+    for(const auto &e : T) if(name && !strcmp(name, e.n)) return e.s;
+    return -1;
+}
+
 extern "C" int sqb_graph_count(void){ return sqb_ngraphs(); }
 extern "C" const char *sqb_graph_name(int i){ const sqb_graph_t *g = sqb_graph_at(i); return g ? g->name : NULL; }
 extern "C" const char *sqb_graph_volkov(const char *name){ const sqb_graph_t *g = sqb_find_graph(name); return g ? g->volkov : NULL; }
@@ -73,7 +85,18 @@ struct Run {
     sqb_opts_t o; sqb_test_t t;
     std::vector<double> X, Wt;
     long nq = 0, unresdrop = 0; double u = 0;
+    sqb_vtab_t *vt = NULL;          /* the predictor's table (opts.predict > 0), else NULL */
 };
+/* releases the predictor's table on every return of sqb_hsum */
+struct VtabGuard { sqb_vtab_t t; VtabGuard(){ memset(&t, 0, sizeof t); } ~VtabGuard(){ sqb_vtab_free(&t, sqb_dev_stream()); } };
+/* the predictor's table must not have overflowed */
+static int vt_check(Run &R, char *err, size_t n){
+    if(!R.vt) return 0;
+    long vn = 0, full = 0;
+    if(sqb_vtab_counts(R.vt, &vn, &full, sqb_dev_stream())){ snprintf(err, n, "predictor: %s", sqb_vtab_error()); return -1; }
+    if(full){ snprintf(err, n, "predictor: %ld values found its table full", full); return -1; }
+    return 0;
+}
 
 static void set_test(Run &R, double abserr){
     R.t.abserr = abserr; R.t.nearf = R.o.nearf; R.t.ddslack = R.o.ddslack;
@@ -146,6 +169,9 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
         if(sqb_dev_eval_resident(R.g, pts, n, skip, &R.t, v.data(), stt.data(), &R.nq, &R.u, &R.unresdrop, &vd, &sd))
             FAIL("device: %s", sqb_last_error());
         if(sqb_grow_shells(cls.data())) FAIL("device grow: %s", sqb_top_error());
+        /* the predictor stores every grow value (driver/sumkey.h:219-222) */
+        if(R.vt && (sqb_vtab_reserve(R.vt, n, sqb_dev_stream()) || sqb_vtab_put_nodes(R.vt, pts, vd, n, R.D, sqb_dev_stream())))
+            FAIL("predictor: %s", sqb_vtab_error());
         const double t1 = now(); te += t1 - t0; nfr++;
         ne += n;
         /* the frontier's sums in point order, then its threshold (driver/sumkey.h:225-245) */
@@ -170,6 +196,12 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
       for(long i = 0; i < nkeep; i++) if(!(kv[i] >= thr)) dr += kv[i]*pw; }
     long m = 0;
     if(sqb_grow_finish(thr, store && R.D < SQB_MAXD, &m)) FAIL("device grow: %s", sqb_top_error());
+    /* ... and what the eps*10^t grows evaluated (driver/sumkey.h:445-451) */
+    if(R.vt && store && R.D < SQB_MAXD && m){
+        const sqb_pt_t *kp; long km;
+        sqb_grow_kept(&kp, &km);
+        if(sqb_vtab_raise_kept(R.vt, kp, km, R.D, st, R.K, sqb_dev_stream())) FAIL("predictor: %s", sqb_vtab_error());
+    }
     const double tg2 = now();
     *dilated = NULL; *ndil = 0;
     if(store && sqb_grow_dilate(nbits, dilated, ndil)) FAIL("device dilate: %s", sqb_top_error());
@@ -216,6 +248,8 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
     /* the symmetry fold's group (driver/sum.c:566-592), before the run's clock starts as there */
     sqb_sym_t sym; memset(&sym, 0, sizeof sym); sym.n = 1;
     res->sym_order = 1;
+    VtabGuard vtg;
+    if(R.o.predict > 0) R.vt = &vtg.t;
     if(R.o.sym && *R.o.sym){
         static thread_local int el[SQB_SYMG*SQB_MAXD];
         const int n = sqb_sym_find(R.D, sym_nodes, &R, R.o.sym, el, res->sym_desc, sizeof res->sym_desc, &res->sym_worst,
@@ -245,7 +279,9 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
     if(resumed){
         for(int i = 0; i < 3; i++) res->S[i] = NAN;
         res->nev = ck.nev; res->ref = ck.ref; res->prune = ck.prune; res->trunc = ck.trunc; res->kept_top = ck.kept_top;
-        R.nq = ck.nq; res->abskipped = ck.cnt[1];
+        R.nq = ck.nq; res->abskipped = ck.cnt[1]; res->pskip = ck.cnt[0];
+        if(R.vt && ck.vcap > 0 && ck.vs && sqb_vtab_upload(R.vt, ck.vs, ck.vcap, ck.vn, sqb_dev_stream())){
+            sqb_ckpt_free(&ck); FAIL("predictor: %s", sqb_vtab_error()); }
         nl = ck.nl; for(int i = 0; i < nl; i++) Slev[i] = ck.Slev[i];
         esok = ck.esok; lev0 = ck.lev; cnext = ck.next; t0 -= ck.t;
         ncur = ck.ncur;
@@ -266,6 +302,7 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
         if(zero){ res->zero = 1; res->t = now() - t0; return 0; }
         GrowOut go;
         if(grow(R, top, eps*1e-3, &go, &dcur, &ncur)) return -1;
+        if(vt_check(R, E_, sizeof E_)){ sqb_dev_free(dcur); return -1; }
         res->nev += go.nev; res->ref = go.A; res->prune = go.drop;
         if(top == 0 && go.gshn) res->prune = fabs(go.gshs);
         if(go.A == 0){ sqb_dev_free(dcur); res->t = now() - t0; res->nq = R.nq; res->unresdrop = R.unresdrop; return 0; }
@@ -288,6 +325,14 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
         L.g = R.g; L.cells = dcur + c0; L.ncell = ncur - c0; L.st = st; L.last = last;
         L.pw = pow(st, R.D); L.thr = eps*res->ref*1e-2; L.t = R.t; L.max_children = R.o.max_children;
         L.sym = &sym;
+        /* the predictor: the level before the last stores its values, the last level uses them
+         * (driver/sum.c:385, 739) */
+        if(R.vt){
+            L.vt = R.vt; L.vput = lev == 1; L.esok = esok;
+            if(last) L.predict = R.o.predict;
+            if(L.vput && sqb_vtab_reserve(R.vt, (ncur - c0) << R.D, sqb_dev_stream())){
+                sqb_dev_free(dcur); sqb_ckpt_free(&ck); FAIL("predictor: %s", sqb_vtab_error()); }
+        }
         if(!last){
             double want = (double)(ncur - c0)*(double)(1L << R.D) + nkeep0;
             double room = 0.35*MEMSHARE*(double)sqb_dev_total_bytes()/sizeof(sqb_pt_t);
@@ -305,7 +350,8 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
         nn += nkeep0;
         Slev[nl++] = ddv(acc.S);
         res->prune += ddv(acc.drop); res->nev += (long)acc.ne; R.nq += (long)acc.nq; R.unresdrop += (long)acc.unres;
-        res->abskipped += (long)acc.skipped;
+        res->abskipped += (long)acc.skipped; res->pskip += (long)acc.pskip;
+        if(vt_check(R, E_, sizeof E_)){ sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); return -1; }
         if(res->nlev < 16){ res->lev_evals[res->nlev] = (long)acc.ne; res->lev_ms[res->nlev] = ms; res->nlev++; }
         if(last){ ah = ddv(acc.A); uu = ddv(acc.u); es1 = ddv(acc.b1); es2 = ddv(acc.b2); }
         if(R.o.verbose) fprintf(stderr, "# %s level step %dh: %ld cells, %llu evals, %llu fallback, %ld kept, %.1f ms\n",
@@ -326,8 +372,18 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
             c.ref = res->ref; c.prune = res->prune; c.trunc = res->trunc; c.t = now() - t0;
             c.nev = res->nev; c.nq = R.nq; c.kept_top = res->kept_top;
             c.ncur = nn; c.cur = (signed char*)host.data();
-            c.cnt[1] = res->abskipped; c.esok = esok;
+            c.cnt[0] = res->pskip; c.cnt[1] = res->abskipped; c.esok = esok;
             c.vsz = SQB_CKPT_VSLOT;
+            /* the predictor's table goes with the checkpoint, so that a resumed run predicts as an unbroken
+             * one (driver/sum.c:68-69) */
+            std::vector<char> vs;
+            if(R.vt && R.vt->tab){
+                long vn = 0, full = 0;
+                vs.resize((size_t)R.vt->cap*SQB_CKPT_VSLOT);
+                if(sqb_vtab_counts(R.vt, &vn, &full, sqb_dev_stream()) || sqb_vtab_download(R.vt, vs.data(), sqb_dev_stream())){
+                    sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); FAIL("predictor: %s", sqb_vtab_error()); }
+                c.vs = vs.data(); c.vcap = R.vt->cap; c.vn = vn;
+            }
             if(sqb_ckpt_save(ckfn, &c) && R.o.verbose) fprintf(stderr, "# warning: could not write checkpoint %s\n", ckfn);
             if(R.o.ckpt_stop){
                 sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck);

@@ -70,6 +70,7 @@ int main(int argc, char **argv){
     if((e = getenv("SQB_FMA"))) o.fma = atoi(e);
     if((e = getenv("SQB_SPLIT"))) o.split = atoi(e);
     o.sym = getenv("SINCQED_SYM");     /* unset: no fold, as the reference's GPU build (driver/sum.c:571) */
+    if((e = getenv("SINCQED_PREDICT"))) o.predict = atof(e);
     /* checkpoints at every level end, on by default as in the reference (driver/main.c:28,184) */
     o.ckpt_every = 600;
     if((e = getenv("SINCQED_CKPT"))) o.ckpt_every = atof(e);
@@ -179,6 +180,7 @@ int main(int argc, char **argv){
         if(R.esok){ double d1 = w*(R.S[0] - R.es1), dd2 = w*(R.es1 - R.es2), rr = d1 != 0 ? dd2/d1 : 0;
             say("# %s eps extrapolation: eps*10 would change the value by %+.3e, eps*100 by a further %+.3e (ratio %.2f)", name, -d1, -dd2, rr);
             if(rr > 1.5) say("; pruning loss left at eps ~ %+.2e (add to the value)\n", d1/(rr - 1)); else say("\n"); }
+        if(o.predict > 0) say("# %s predictor alpha %g: skipped %ld final-level points\n", name, o.predict, R.pskip);
         say("# %s timing: top level %.2fs on the host, levels %.2fs", name, R.t_top, R.t_levels);
         for(int l = 0; l < R.nlev; l++) say("%s%ld evals %.1f ms", l ? ", " : " (", R.lev_evals[l], R.lev_ms[l]);
         say("%s\n", R.nlev ? ")" : "");

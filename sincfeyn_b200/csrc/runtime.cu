@@ -64,6 +64,7 @@ typedef struct {
     const double *v, *uu;
     const unsigned char *stt;
     sqb_sym_t sym;                /* the symmetry fold (sym.n <= 1: off) */
+    const unsigned char *cfl;     /* the predictor's per-child tiers at the last level (NULL: the parent's) */
 } lvl_t;
 
 struct Dev {
@@ -77,7 +78,7 @@ struct Dev {
     cudaEvent_t e0, e1;
     double *X, *Wt; int tabcap, K;
     long cap;                      /* points per batch */
-    double *v, *uu; unsigned char *stt; long *fb; unsigned long long *nfb;
+    double *v, *uu; unsigned char *stt, *cfl; long *fb; unsigned long long *nfb;
     long nbcap; part_t *bp; unsigned *bkeep; unsigned long long *boff; unsigned char *tfb;
     long ttcap; double *tt, *ta;   /* split FP64 pass: running sums per point */
     sqb_acc_t *acc; unsigned long long *base;
@@ -153,9 +154,9 @@ extern "C" int sqb_dev_tables(const double *X, const double *Wt, int K){
 static int reserve_points(long n){
     if(n <= G.cap) return 0;
     long c = 1L << 16; while(c < n) c <<= 1;
-    if(G.v){ cudaFree(G.v); cudaFree(G.uu); cudaFree(G.stt); cudaFree(G.fb); cudaFree(G.bp); cudaFree(G.bkeep); cudaFree(G.boff); cudaFree(G.tfb); }
+    if(G.v){ cudaFree(G.v); cudaFree(G.uu); cudaFree(G.stt); cudaFree(G.cfl); cudaFree(G.fb); cudaFree(G.bp); cudaFree(G.bkeep); cudaFree(G.boff); cudaFree(G.tfb); }
     CKR(cudaMalloc(&G.v, c*sizeof(double))); CKR(cudaMalloc(&G.uu, c*sizeof(double)));
-    CKR(cudaMalloc(&G.stt, c)); CKR(cudaMalloc(&G.fb, c*sizeof(long)));
+    CKR(cudaMalloc(&G.stt, c)); CKR(cudaMalloc(&G.cfl, c)); CKR(cudaMalloc(&G.fb, c*sizeof(long)));
     long nb = (c + RTILE - 1)/RTILE;
     CKR(cudaMalloc(&G.bp, nb*sizeof(part_t))); CKR(cudaMalloc(&G.bkeep, nb*sizeof(unsigned))); CKR(cudaMalloc(&G.tfb, nb));
     CKR(cudaMalloc(&G.boff, nb*sizeof(unsigned long long)));
@@ -379,6 +380,7 @@ __device__ __forceinline__ int child_weight(const lvl_t &a, long i){
 }
 
 __device__ __forceinline__ int parent_tier(const lvl_t &a, long i){
+    if(a.cfl) return (a.cfl[i] >> 1) & 3;
     const long c = i >> a.D;
     return (a.cells[c*SQB_MAXD + SQB_PFLAG] >> 1) & 3;
 }
@@ -570,6 +572,13 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
         if(!L->t.alldd && can0 && round > 0 && ncb >= 2*round) ncb = (ncb/round)*round;
     }
     if(reserve_points(ncb << D)) return -1;
+    /* the predictor runs at the last level when its table holds values (driver/sum.c:385) */
+    bool pon = false;
+    if(L->last && L->predict > 0 && L->vt && L->vt->tab){
+        long vn = 0, full = 0;
+        if(sqb_vtab_counts(L->vt, &vn, &full, G.s)){ snprintf(g_err, sizeof g_err, "%s", sqb_vtab_error()); return -1; }
+        pon = vn > 0;
+    }
     CKR(cudaMemsetAsync(G.acc, 0, sizeof(sqb_acc_t), G.s));
     CKR(cudaEventRecord(G.e0, G.s));
     for(long c0 = 0; c0 < L->ncell; c0 += ncb){
@@ -588,12 +597,25 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
         int can = 0;
         const long cap = grid_cap(g, f64_which(g, L->t.fma), 2*(2*G.K + 1)*sizeof(double), &can);
         const bool fused = !L->t.alldd && can && !use_split(g, &a, &L->t) && nch >= 2*SQB_TILE*cap;
+        /* the predictor at the last level: which children to leave out, and their tiers */
+        if(pon){
+            if(sqb_vtab_predict(L->vt, cells, nc, D, L->st, G.K, L->thr, L->predict, L->esok, L->sym, G.cfl,
+                                &G.acc->pskip, G.nsm, G.s)){ snprintf(g_err, sizeof g_err, "%s", sqb_vtab_error()); return -1; }
+            G.launches++;
+            a.cfl = G.cfl;
+        }
         if(fused){ a.part = G.bp; a.tkeep = G.bkeep; a.tfb = G.tfb; a.pw = L->pw; a.thr = L->thr; a.last = L->last; }
         if(eval_batch(g, &a, &L->t, nch)) return -1;
         lvl_t r; memset(&r, 0, sizeof r);
         r.cells = (const signed char*)cells; r.n = nch; r.D = D; r.st = L->st; r.last = L->last;
         r.abskip = L->t.abskip; r.pw = L->pw; r.thr = L->thr; r.v = G.v; r.uu = G.uu; r.stt = G.stt;
-        r.sym = a.sym;
+        r.sym = a.sym; r.cfl = a.cfl;
+        /* the level before the last stores its values for the predictor */
+        if(L->vput && L->vt){
+            if(sqb_vtab_put_children(L->vt, cells, nch, D, L->st, G.v, G.stt, L->sym, G.s)){
+                snprintf(g_err, sizeof g_err, "%s", sqb_vtab_error()); return -1; }
+            G.launches++;
+        }
         const long nb = (nch + RTILE - 1)/RTILE;
         sqb_k_reduce<<<(unsigned)nb, RT, 0, G.s>>>(r, G.bp, G.bkeep, fused ? G.tfb : NULL);
         CKR(cudaGetLastError());
@@ -615,6 +637,7 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
     double *src[6] = {h.S, h.A, h.drop, h.b1, h.b2, h.u}, *dst[6] = {acc->S, acc->A, acc->drop, acc->b1, acc->b2, acc->u};
     for(int q = 0; q < 6; q++){ sqdd x = sqdd(dst[q][0], dst[q][1]) + sqdd(src[q][0], src[q][1]); dst[q][0] = x.hi; dst[q][1] = x.lo; }
     acc->ne += h.ne; acc->nq += h.nq; acc->unres += h.unres; acc->skipped += h.skipped; acc->keep += h.keep; acc->overflow += h.overflow;
+    acc->pskip += h.pskip;
     *next_n = (long)h.keep;
     return 0;
 }

@@ -66,6 +66,8 @@ typedef struct {
     double pw, thr;               /* the level's weight step^D and keep threshold */
     int last;                     /* the last level: shadow-tier sums, no kept children */
     sqb_sym_t sym;                /* cells only: the symmetry fold (sym.n <= 1: off) */
+    const unsigned char *cfl;     /* cells only, the predictor at the last level (NULL: off): per child, bit 0 =
+                                     not evaluated, bits 1-2 = its shadow tier */
 } sqb_eval_t;
 
 /* The double-double kernel over a list of points of the same launch geometry (fb/nfb from the FP64

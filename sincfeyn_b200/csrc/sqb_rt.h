@@ -24,7 +24,28 @@ typedef struct {
 typedef struct {
     double S[2], A[2], drop[2], b1[2], b2[2], u[2];
     unsigned long long ne, keep, nq, unres, skipped, overflow;
+    unsigned long long pskip;           /* last level: children the predictor left out */
 } sqb_acc_t;
+
+/* the predictor's table of step-2h values (predict.cu): device slots, capacity (a power of two), and
+ * two device counters (keys stored, inserts that found the table full) */
+typedef struct {
+    void *tab; long cap;
+    unsigned long long *vn, *full;
+} sqb_vtab_t;
+int  sqb_vtab_reserve(sqb_vtab_t *t, long more, void *stream);
+int  sqb_vtab_put_nodes(sqb_vtab_t *t, const sqb_pt_t *pts, const double *v, long n, int D, void *stream);
+int  sqb_vtab_raise_kept(sqb_vtab_t *t, const sqb_pt_t *keep, long m, int D, int st, int K, void *stream);
+int  sqb_vtab_put_children(sqb_vtab_t *t, const void *cells, long nch, int D, int st, const double *v,
+                           const unsigned char *stt, const sqb_sym_t *sym, void *stream);
+int  sqb_vtab_predict(const sqb_vtab_t *t, const void *cells, long ncell, int D, int st, int K, double thr,
+                      double alpha, int esok, const sqb_sym_t *sym, unsigned char *cfl,
+                      unsigned long long *pskip, int nsm, void *stream);
+int  sqb_vtab_counts(const sqb_vtab_t *t, long *vn, long *full, void *stream);
+int  sqb_vtab_download(const sqb_vtab_t *t, void *host, void *stream);
+int  sqb_vtab_upload(sqb_vtab_t *t, const void *host, long cap, long vn, void *stream);
+void sqb_vtab_free(sqb_vtab_t *t, void *stream);
+const char *sqb_vtab_error(void);
 
 const sqb_graph_t *sqb_find_graph(const char *name);
 int  sqb_ngraphs(void);
@@ -54,6 +75,10 @@ typedef struct {
     sqb_test_t t;
     long max_children;                  /* children per batch (0: default) */
     const sqb_sym_t *sym;               /* the symmetry fold (NULL or n <= 1: off) */
+    /* the predictor: vput = store this level's values in vt (the level before the last); predict > 0 at
+     * the last level = leave out the children whose predicted mean is below predict*thr (esok: and cap
+     * their tiers) */
+    sqb_vtab_t *vt; int vput; double predict; int esok;
 } sqb_level_t;
 int  sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n, double *ms);
 
@@ -72,6 +97,7 @@ int  sqb_grow_expand(const double *v_dev, const unsigned char *stt_dev, double t
 int  sqb_grow_kv(double *kv_host, long n);
 int  sqb_grow_finish(double thr, int tiers, long *m);
 int  sqb_grow_dilate(int nbits, sqb_pt_t **out, long *n);
+void sqb_grow_kept(const sqb_pt_t **keep, long *m);
 void sqb_grow_end(void);
 const char *sqb_top_error(void);
 int  sqb_radix_sort_u64(unsigned long long *keys_dev, long n, int nbits, void *stream);

@@ -70,9 +70,9 @@ __device__ __forceinline__ int sqb_orbit(const sqb_sym_t &s, const int (&k)[D]){
     return s.n/stab;
 }
 
-/* coordinates and weight of point i; returns 0 for a child below the box or, under a symmetry fold, a
- * child that is not the minimum of its orbit (driver/sum.c:405-409), else the point's multiplicity
- * (the orbit size; 1 without a fold) */
+/* coordinates and weight of point i; returns 0 for a child below the box, a child the predictor leaves
+ * out or, under a symmetry fold, a child that is not the minimum of its orbit (driver/sum.c:405-416), else
+ * the point's multiplicity (the orbit size; 1 without a fold) */
 template<int D>
 __device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const double *sX, const double *sW,
                                          long i, long *cell, double *sf, double *w){
@@ -108,6 +108,7 @@ __device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const double *sX, 
     }
     *w = ww;
     if(!in) return 0;
+    if(a.cfl && (a.cfl[i] & 1)) return 0;          /* left out by the predictor */
     return a.cells && a.sym.n > 1 ? sqb_orbit<D>(a.sym, kk) : 1;
 }
 
@@ -249,7 +250,8 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const sqb_eval_
                 const double m = (double)mw, vp = (m*v)*a.pw, av = fabs(v);
                 sqb_acc_dd(ta.S, t, vp); ta.A[t] += m*av; ta.ne[t]++; ta.nsk[t] += sk ? 1 : 0;
                 if(a.last){
-                    const int te = (((const signed char*)a.pts)[c*(long)a.stride + a.flag_at] >> 1) & 3;
+                    const int te = a.cfl ? (a.cfl[i] >> 1) & 3
+                                         : (((const signed char*)a.pts)[c*(long)a.stride + a.flag_at] >> 1) & 3;
                     if(te >= 1) sqb_acc_dd(ta.b1, t, vp);
                     if(te >= 2) sqb_acc_dd(ta.b2, t, vp);
                 } else if(av >= a.thr) ta.keep[t] += mw;

@@ -585,6 +585,9 @@ extern "C" int sqb_grow_dilate(int nbits, sqb_pt_t **out, long *n){
     }
 }
 
+/* the kept list after sqb_grow_finish (tiers in the flag byte), on the device */
+extern "C" void sqb_grow_kept(const sqb_pt_t **keep, long *m){ *keep = GR.keep; *m = GR.nkeep; }
+
 /* top = 0 keeps no list; the kept list is released with the table */
 extern "C" void sqb_grow_end(void){
     if(GR.key){ DFREE(GR.key); DFREE(GR.word); GR.key = NULL; }

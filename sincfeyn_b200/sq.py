@@ -24,7 +24,7 @@ class Opts(C.Structure):
                 ('abskip', C.c_int), ('abcheck', C.c_int), ('dropunres', C.c_int), ('growskip', C.c_int),
                 ('alldd', C.c_int), ('device', C.c_int), ('max_children', C.c_long), ('verbose', C.c_int),
                 ('ckpt_every', C.c_double), ('ckpt_dir', C.c_char_p), ('ckpt_stop', C.c_int), ('fma', C.c_int),
-                ('split', C.c_int), ('sym', C.c_char_p)]
+                ('split', C.c_int), ('sym', C.c_char_p), ('predict', C.c_double)]
 
 
 class Result(C.Structure):
@@ -38,7 +38,7 @@ class Result(C.Structure):
                 ('lev_evals', C.c_long * 16), ('lev_ms', C.c_double * 16),
                 ('f64_ms', C.c_double), ('dd_ms', C.c_double), ('f64_launches', C.c_long), ('launches', C.c_long),
                 ('sym_order', C.c_int), ('sym_desc', C.c_char * 256), ('sym_worst', C.c_double),
-                ('sym_msg', C.c_char * 512)]
+                ('sym_msg', C.c_char * 512), ('pskip', C.c_long)]
 
 
 class ScaleResult(C.Structure):

@@ -24,13 +24,16 @@ Fixtures
   scale.json                    `sincqed scale SEL kappa seed` of the -ffp-contract=off build, one thread
                                 (directions in order): the stdout lines per graph, kappa = 24 for all2, g3_00,
                                 g3_07, g3_lbl, v3_00 and kappa = 3 (slow directions listed) for g2_00, g3_07
+  predict.json                  the last-level predictor, SINCQED_PREDICT=1 (driver/sum.c:64-69, 379-422), the
+                                -ffp-contract=off build with SINCQED_KEEPBT=1: runs unfolded (SINCQED_SYM=0) and
+                                one folded, with the log's count of final-level points left out
   fold.json                     the symmetry fold (driver/sum.c:21-46, 464-592), -ffp-contract=off build:
                                 the group line the reference prints for every graph of g2 g3 v3 v4 w4
                                 (`run 2.0 13 1e-4 GRAPH`, SINCQED_SYM unset = auto; the search's nodes only
                                 need K >= 6), and folded sums (SINCQED_SYM unset, SINCQED_KEEPBT=1) with
                                 top = 2 so that kept orbits go on to a second refinement level
 
-    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold scale]   # default: all of them
+    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold scale predict]   # default: all of them
 """
 import json
 import os
@@ -146,6 +149,26 @@ def scale():
         json.dump(d, f, indent=1)
 
 
+PREDICT_RUNS = [('g2_01', 0.7, 139, '0'), ('g2_03', 0.7, 139, '0'), ('v2_00', 0.7, 139, '0'), ('g3_07', 0.7, 139, '0'),
+                ('v3_01', 0.7, 139, '0'), ('g3_25', 1.0, 97, '0'), ('g3_07', 0.7, 139, None)]
+
+
+def predict():
+    d = {'alpha': 1.0, 'eps': 1e-12, 'runs': []}
+    for name, h, N, sym in PREDICT_RUNS:
+        env = {'SINCQED_PREDICT': '1', 'SINCQED_KEEPBT': '1'}
+        if sym is not None:
+            env['SINCQED_SYM'] = sym
+        rows, out = refpy.run(refpy.SINCQED_EXACT, h, N, 1e-12, [name], top=2, env=env)
+        r = with_log(rows, out)[0]
+        r.pop('time_s', None)
+        m = re.search(r'^# %s predictor alpha \S+: skipped (\d+) final-level points' % re.escape(name), out, re.M)
+        r.update(h=h, N=N, top=2, fold=sym is None, pskip=int(m.group(1)))
+        d['runs'].append(r)
+    with open(os.path.join(OUT, 'predict.json'), 'w') as f:
+        json.dump(d, f, indent=1)
+
+
 def fold():
     h, N, eps = FOLD_GROUP_RUN
     d = {'group_run': {'h': h, 'N': N, 'eps': eps}, 'groups': {}, 'runs': [], 'env': {'SINCQED_KEEPBT': '1'}}
@@ -165,7 +188,7 @@ def fold():
 
 
 if __name__ == '__main__':
-    parts = sys.argv[1:] or ['all2', 'boxsum', 'pointwise', 'synth', 'fold', 'scale']
+    parts = sys.argv[1:] or ['all2', 'boxsum', 'pointwise', 'synth', 'fold', 'scale', 'predict']
     if 'all2' in parts:
         all2()
     if 'boxsum' in parts:
@@ -182,3 +205,5 @@ if __name__ == '__main__':
         fold()
     if 'scale' in parts:
         scale()
+    if 'predict' in parts:
+        predict()

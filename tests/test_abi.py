@@ -50,3 +50,21 @@ def test_selectors_match_the_reference_groups():
 def test_default_top_follows_the_reference():
     assert sq.default_top(1.0) == 1 and sq.default_top(0.9) == 1 and sq.default_top(0.8) == 1
     assert sq.default_top(0.7) == 2 and sq.default_top(0.75) == 2
+
+
+def test_struct_mirrors_have_the_library_sizes():
+    """the ctypes copies of the interface's structures (sincfeyn_b200/sq.py, and the level interface the
+    no-alloc test drives) have the sizes the library was compiled with"""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import test_zz_no_alloc as na
+    from test_codegen_host import ScaleArgs
+    L = sq.lib()
+    L.sqb_struct_size.argtypes = [C.c_char_p]
+    L.sqb_struct_size.restype = C.c_long
+    for name, cls in (('sqb_opts_t', sq.Opts), ('sqb_result_t', sq.Result), ('sqb_job_t', sq.Job),
+                      ('sqb_ckpt_t', sq.Checkpoint), ('sqb_scale_result_t', sq.ScaleResult),
+                      ('sqb_level_t', na.Level), ('sqb_acc_t', na.Acc), ('sqb_test_t', na.PointTestParams),
+                      ('sqb_scale_t', ScaleArgs)):
+        assert L.sqb_struct_size(name.encode()) == C.sizeof(cls), name
+    assert L.sqb_struct_size(b'no_such_struct') == -1

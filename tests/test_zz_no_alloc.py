@@ -29,15 +29,19 @@ class PointTestParams(C.Structure):
 
 
 class Level(C.Structure):
+    """sqb_level_t (sqb_rt.h), every field: no fold, no predictor"""
     _fields_ = [('g', C.c_void_p), ('cells', C.c_void_p), ('ncell', C.c_long), ('next', C.c_void_p),
                 ('next_cap', C.c_long), ('st', C.c_int), ('last', C.c_int), ('pw', C.c_double), ('thr', C.c_double),
-                ('t', PointTestParams), ('max_children', C.c_long)]
+                ('t', PointTestParams), ('max_children', C.c_long), ('sym', C.c_void_p), ('vt', C.c_void_p),
+                ('vput', C.c_int), ('predict', C.c_double), ('esok', C.c_int)]
 
 
 class Acc(C.Structure):
+    """sqb_acc_t (sqb_rt.h), every field"""
     _fields_ = [('S', C.c_double * 2), ('A', C.c_double * 2), ('drop', C.c_double * 2), ('b1', C.c_double * 2),
                 ('b2', C.c_double * 2), ('u', C.c_double * 2), ('ne', C.c_ulonglong), ('keep', C.c_ulonglong),
-                ('nq', C.c_ulonglong), ('unres', C.c_ulonglong), ('skipped', C.c_ulonglong), ('overflow', C.c_ulonglong)]
+                ('nq', C.c_ulonglong), ('unres', C.c_ulonglong), ('skipped', C.c_ulonglong), ('overflow', C.c_ulonglong),
+                ('pskip', C.c_ulonglong)]
 
 
 def cells_box():
