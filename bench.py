@@ -39,7 +39,8 @@ Other measurements (one GPU, each prints its own JSON lines; not the headline):
   --workload synth   the synthetic Sinc-sum microbenchmark (d = 5, 8, 11; h = 1.0, 0.7) and its
                      precision table (FP64 only, FP64 + dd, all-dd, the reference's hsum)
   --workload vp4     the four-loop lepton-loop set (kernels/v4, kernels/w4) at h = 1.0 and 0.9, with the
-                     exactly known set values (--fold: with the symmetry fold)
+                     exactly known set values (--fold: with the symmetry fold; --predict alpha: with the
+                     last-level predictor)
   --workload single  one integral (--graph) warm, then timed once: a small command for profilers
   --workload points  one launch of a graph's evaluation kernel on --npoints seeded nodes (--prec)
 """
@@ -246,7 +247,8 @@ def run_vp4(args, sq, L):
         if args.vp4_h and h not in args.vp4_h:
             continue
         jobs = [(g, h, N, EPS, -1, (2.0/h)**info[g]['D']) for g in names]
-        res, ms = sq.hsum_batch(jobs, workers=workers, **({'sym': 'auto'} if args.fold else {}))
+        kw = dict(({'sym': 'auto'} if args.fold else {}), **({'predict': args.predict} if args.predict > 0 else {}))
+        res, ms = sq.hsum_batch(jobs, workers=workers, **kw)
         nev = sum(r['nev'] for r in res)
         val = {g: r['S'][0]*info[g]['weight'] for g, r in zip(names, res)}
         sets = []
@@ -256,6 +258,7 @@ def run_vp4(args, sq, L):
             sets.append({'set': label, 'graphs': len(mem), 'sum': s, 'exact': exact, 'diff': s - exact})
         slow = sorted(zip(names, res), key=lambda x: -x[1]['t'])[:5]
         row = {'h': h, 'N': N, 'integrals': len(jobs), 'workers': workers, 'fold': bool(args.fold),
+               'predict': args.predict, 'predicted_out': sum(r['pskip'] for r in res),
                'device_s': ms*1e-3, 'points': nev,
                'points_s': nev/(ms*1e-3), 'fallback': sum(r['nq'] for r in res), 'sets': sets,
                'slowest': [[g, round(r['t'], 2), r['nev']] for g, r in slow],
@@ -364,6 +367,7 @@ def main():
     ap.add_argument('--alldd-full', action='store_true', help='all-double-double comparison on the whole set (~2 min)')
     ap.add_argument('--no-fold', action='store_true', help='skip the batch with the symmetry fold')
     ap.add_argument('--fold', action='store_true', help='--workload vp4: with the symmetry fold (sym=auto)')
+    ap.add_argument('--predict', type=float, default=0.0, help='--workload vp4: the last-level predictor with this alpha')
     ap.add_argument('--workers', type=int, default=0, help='batch workers for --workload vp4 (default 6)')
     ap.add_argument('--vp4-h', type=float, action='append', help='--workload vp4: only these h (repeatable)')
     ap.add_argument('--graph', default='g3_00', help='--workload single/points: the graph')
