@@ -230,9 +230,9 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     graphs = generate(srcs)
     flops = count_flops(graphs)
     reg = write_registry(graphs, flops)
-    hdrs = [os.path.join(CSRC, f) for f in ('sqkern.cuh', 'sqdd.cuh', 'sqscale.cuh', 'sqb_internal.h', 'sqb_rt.h')] + \
+    hdrs = [os.path.join(CSRC, f) for f in ('sqkern.cuh', 'sqdd.cuh', 'sqscale.cuh', 'sqorbit.cuh', 'sqb_internal.h', 'sqb_rt.h')] + \
            [os.path.join(INC, 'sincfeyn_b200.h')]
-    khdrs = [os.path.join(CSRC, f) for f in ('sqkern.cuh', 'sqdd.cuh', 'sqscale.cuh', 'sqb_internal.h')]   # what a graph TU includes
+    khdrs = [os.path.join(CSRC, f) for f in ('sqkern.cuh', 'sqdd.cuh', 'sqscale.cuh', 'sqorbit.cuh', 'sqb_internal.h')]   # what a graph TU includes
     jobs_list = []
     for name, D, cuh, tu in graphs:
         o = os.path.join(OBJ, 'k_%s.o' % name)

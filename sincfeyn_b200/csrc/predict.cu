@@ -22,6 +22,7 @@
 #include <stdio.h>
 #include <string.h>
 #include "sqb_rt.h"
+#include "sqorbit.cuh"
 
 struct VSlot { unsigned long long k; float v; unsigned t; };   /* the reference's vslot_t bytes (t < 256) */
 static_assert(sizeof(VSlot) == 16, "one slot is 16 bytes, as the checkpoint stores it");
@@ -109,7 +110,6 @@ __global__ void k_vraise_kept(const sqb_pt_t *keep, long m, int D, int st, int K
 __global__ void k_vput_children(const signed char *cells, long nch, int D, int st, const double *v,
                                 const unsigned char *stt, sqb_sym_t sym, VSlot *T, long cap,
                                 unsigned long long *vn, unsigned long long *full){
-    const unsigned uD = (unsigned)D;
     for(long i = blockIdx.x*(long)blockDim.x + threadIdx.x; i < nch; i += (long)gridDim.x*blockDim.x){
         if(!(stt[i] & SQB_PRESENT)) continue;
         const long c = i >> D; const int b = (int)(i & ((1L << D) - 1));
@@ -120,14 +120,8 @@ __global__ void k_vput_children(const signed char *cells, long nch, int D, int s
         const float lv = v_log(fabs(v[i]));
         const int ng = sym.n > 1 ? sym.n : 1;
         for(int e = 0; e < ng; e++){
-            bool dup = false;
-            for(int f = 0; f < e && !dup; f++){
-                bool eq = true;
-                for(int d = 0; d < D && eq; d++) eq = k[(unsigned)sym.g[e][d] % uD] == k[(unsigned)sym.g[f][d] % uD];
-                dup = eq;
-            }
-            if(dup) continue;
-            for(int d = 0; d < D; d++) im[d] = e ? k[(unsigned)sym.g[e][d] % uD] : k[d];
+            if(!sqb_image_new(sym, k, D, e)) continue;
+            sqb_image(sym, k, D, e, im);
             v_put(T, cap, v_hash(im, D), lv, t, vn, full);
         }
     }
@@ -146,7 +140,6 @@ __global__ void __launch_bounds__(32) k_predict(const signed char *cells, long n
     extern __shared__ double pm[];
     const int nc = 1 << D, l = threadIdx.x;
     double *s0 = pm, *s1 = pm + nc, *s2 = pm + 2*nc;
-    const unsigned uD = (unsigned)D;
     for(long c = blockIdx.x; c < ncell; c += gridDim.x){
         const signed char *p = cells + c*SQB_MAXD;
         int kp[SQB_MAXD];
@@ -180,12 +173,7 @@ __global__ void __launch_bounds__(32) k_predict(const signed char *cells, long n
             for(int d = 0; d < D; d++){ k[d] = kp[d] - (((b >> d) & 1) ? st : 0); if(k[d] < -K) in = false; }
             unsigned char out = (unsigned char)(tp << 1);
             if(in){
-                bool canon = true;
-                for(int e = 1; e < sym.n && canon; e++){
-                    int cmp = 0;
-                    for(int i = 0; i < D && !cmp; i++){ const int x = k[i], y = k[(unsigned)sym.g[e][i] % uD]; if(x != y) cmp = x < y ? -1 : 1; }
-                    canon = cmp <= 0;
-                }
+                const bool canon = sym.n <= 1 || sqb_orbit_n(sym, k, D) > 0;
                 if(canon && s0[b] < alpha*thr){ out = 1; nsk++; }
                 else if(canon && esok){
                     const int tq = (s1[b] >= alpha*10*thr) + (s1[b] >= alpha*10*thr && s2[b] >= alpha*100*thr);

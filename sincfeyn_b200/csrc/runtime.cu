@@ -22,6 +22,7 @@
 #include <omp.h>
 #include "sqb_rt.h"
 #include "sqdd.cuh"
+#include "sqorbit.cuh"
 #include <atomic>
 #include <vector>
 #include "sincfeyn_b200.h"
@@ -359,24 +360,12 @@ __device__ __forceinline__ void child_of(const lvl_t &a, long i, int *k){
     const signed char *p = a.cells + c*SQB_MAXD;
     for(int d = 0; d < a.D; d++) k[d] = p[d] - (((b >> d) & 1) ? a.st : 0);
 }
-/* the image of k under group element e (symimg(), driver/sum.c:29) is k'_i = k[g[e][i]]; 0 if k is not
- * the minimum of its orbit, else the orbit size (symw(), driver/sum.c:30-37) */
-__device__ int orbit_size(const sqb_sym_t &s, const int *k, int D){
-    int stab = 1;
-    for(int e = 1; e < s.n; e++){
-        int c = 0;
-        for(int i = 0; i < D && !c; i++){ const int x = k[i], y = k[(unsigned)s.g[e][i] % (unsigned)D]; if(x != y) c = x < y ? -1 : 1; }
-        if(c > 0) return 0;
-        if(!c) stab++;
-    }
-    return s.n/stab;
-}
 /* a present child's multiplicity: its orbit size under a fold, else 1 */
 __device__ __forceinline__ int child_weight(const lvl_t &a, long i){
     if(a.sym.n <= 1) return 1;
     int k[SQB_MAXD];
     child_of(a, i, k);
-    return orbit_size(a.sym, k, a.D);
+    return sqb_orbit_n(a.sym, k, a.D);
 }
 
 __device__ __forceinline__ int parent_tier(const lvl_t &a, long i){
@@ -536,19 +525,14 @@ __global__ void __launch_bounds__(RT) sqb_k_scatter(const lvl_t a, const unsigne
         /* the child, then (under a fold) the other members of its orbit in group order, each once
          * (symorbit(), driver/sum.c:38-46), all with the child's flags (driver/sum.c:741-744) */
         const int ng = a.sym.n > 1 ? a.sym.n : 1;
-        const unsigned uD = (unsigned)a.D;
         for(int e = 0; e < ng; e++){
-            bool dup = false;
-            for(int f = 0; f < e && !dup; f++){
-                bool eq = true;
-                for(int d = 0; d < a.D && eq; d++) eq = k[(unsigned)a.sym.g[e][d] % uD] == k[(unsigned)a.sym.g[f][d] % uD];
-                dup = eq;
-            }
-            if(dup) continue;
+            if(!sqb_image_new(a.sym, k, a.D, e)) continue;
             if((long)o >= cap){ atomicAdd(overflow, 1ULL); o++; continue; }
             union { signed char k[SQB_MAXD]; int w[3]; } q;
             q.w[0] = q.w[1] = q.w[2] = 0;
-            for(int d = 0; d < a.D; d++) q.k[d] = (signed char)(e ? k[(unsigned)a.sym.g[e][d] % uD] : k[d]);
+            int im[SQB_MAXD];
+            sqb_image(a.sym, k, a.D, e, im);
+            for(int d = 0; d < a.D; d++) q.k[d] = (signed char)im[d];
             q.k[SQB_PFLAG] = fl;
             int *dst = (int*)(next + o);
             dst[0] = q.w[0]; dst[1] = q.w[1]; dst[2] = q.w[2];

@@ -20,6 +20,7 @@
 #include "sqdd.cuh"
 #include "sqb_internal.h"
 #include "sqscale.cuh"
+#include "sqorbit.cuh"
 
 #ifndef SQG_NS
 #define SQG_NS(n) sqg_##n                    /* the graph's namespace (sqgf_<name> in the contracted unit) */
@@ -47,28 +48,6 @@
                                  that spills its registers is built without it, keeping L1 for its stack */
 #endif
 #define SQB_QEPS 4.93e-32   /* double-double epsilon of the fallback's error model (driver/common.h:8) */
-
-/* The symmetry fold's test (symw(), driver/sum.c:30-37): 0 if k is not the lexicographic minimum of
- * its orbit under the group, else the orbit size n / |stabiliser|.  The image k[g[e][i]] is selected
- * from the registers by an unrolled compare, so k stays out of local memory. */
-template<int D>
-__device__ __forceinline__ int sqb_orbit(const sqb_sym_t &s, const int (&k)[D]){
-    int stab = 1;
-    for(int e = 1; e < s.n; e++){
-        int c = 0;
-#pragma unroll
-        for(int i = 0; i < D; i++){
-            const int p = s.g[e][i];
-            int y = k[0];
-#pragma unroll
-            for(int j = 1; j < D; j++) y = p == j ? k[j] : y;
-            if(c == 0 && k[i] != y) c = k[i] < y ? -1 : 1;
-        }
-        if(c > 0) return 0;
-        if(c == 0) stab++;
-    }
-    return s.n/stab;
-}
 
 /* coordinates and weight of point i; returns 0 for a child below the box, a child the predictor leaves
  * out or, under a symmetry fold, a child that is not the minimum of its orbit (driver/sum.c:405-416), else
