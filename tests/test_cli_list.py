@@ -1,0 +1,25 @@
+"""The graph registry as the command line shows it (CPU, no device): `sincqed list` of the evaluator and of
+the reference build (oracle/_ref/sincqed, driver/main.c:186-190) print the same graphs in the same order
+with the same Volkov strings, loop counts, dimensions and mirror weights (the registry of
+driver/graphs.c:8-12, first name wins)."""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+OURS = os.path.join(ROOT, 'sincfeyn_b200', 'bin', 'sincqed')
+REF = os.path.join(ROOT, 'oracle', '_ref', 'sincqed')
+
+
+def graph_lines(binary):
+    out = subprocess.run([binary, 'list'], stdout=subprocess.PIPE, text=True, check=True, timeout=120).stdout
+    return [ln for ln in out.splitlines() if ln.startswith('  ')]
+
+
+def test_list_matches_the_reference():
+    if not (os.path.exists(OURS) and os.path.exists(REF)):
+        pytest.skip('build first (python -m sincfeyn_b200.build; make -C oracle)')
+    ours, ref = graph_lines(OURS), graph_lines(REF)
+    assert len(ours) >= 170
+    assert ours == ref
