@@ -43,3 +43,14 @@ def test_compare_matches_the_reference(tmp_path):
         got = subprocess.run([OURS, 'compare', a, b], stdout=subprocess.PIPE, text=True, check=True).stdout
         assert got == want
         assert want.count('\n') >= 5
+
+
+@pytest.mark.parametrize('sel', ['vp3', 'vp4', 'VP: 1-loop vertex + Pi2 Pi2', 'v4_00'])
+def test_selection_matches_the_reference(sel):
+    """graph selection by group, Volkov string and name (driver/graphs.c:15-29): `sincqed scale SEL` over
+    graphs without a raw point function reports each selected graph without a device, in the same order"""
+    if not (os.path.exists(OURS) and os.path.exists(REF)):
+        pytest.skip('build first (python -m sincfeyn_b200.build; make -C oracle)')
+    want = subprocess.run([REF, 'scale', sel], stdout=subprocess.PIPE, text=True, check=True, timeout=120).stdout
+    got = subprocess.run([OURS, 'scale', sel], stdout=subprocess.PIPE, text=True, check=True, timeout=120).stdout
+    assert got == want and want.count('(no scale test') >= 1
