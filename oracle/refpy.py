@@ -20,6 +20,7 @@ SINCQED = os.path.join(REF_DIR, 'sincqed')
 SINCQED_EXACT = os.path.join(REF_DIR, 'sincqed-exact')
 SINCQED_DROPIN = os.path.join(REF_DIR, 'sincqed-dropin')
 LIBSQREF = os.path.join(REF_DIR, 'libsqref.so')
+LIBSQREF_PI6 = os.path.join(REF_DIR, 'libsqref_pi6.so')   # the pi6 class alone
 BOXSUM = os.path.join(REF_DIR, 'boxsum_gl')
 
 COLS = ['name', 'volkov', 'L', 'D', 'w', 'h', 'N', 'eps', 'top', 'value', 'err', 'disc', 'prune', 'trunc',
@@ -72,13 +73,14 @@ def run(binary, h, N, eps, graphs, top=None, env=None, timeout=3600, threads=Non
             return parse_results(f.read()), out.stdout
 
 
-_lib = None
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        L = C.CDLL(LIBSQREF)
+def lib(path=None):
+    """the kernels' shim library (default libsqref.so; LIBSQREF_PI6 for the pi6 class)"""
+    path = path or LIBSQREF
+    if path not in _libs:
+        L = C.CDLL(path)
         L.sqref_info.argtypes = [C.c_char_p, C.POINTER(C.c_int)]
         for fn in (L.sqref_fd, L.sqref_fv):
             fn.argtypes = [C.c_char_p, C.c_long, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
@@ -86,26 +88,26 @@ def lib():
         L.sqref_name.restype = C.c_char_p
         L.sqref_volkov.restype = C.c_char_p
         L.sqref_volkov.argtypes = [C.c_char_p]
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
-def names():
-    L = lib()
+def names(path=None):
+    L = lib(path)
     return [L.sqref_name(i).decode() for i in range(L.sqref_count())]
 
 
-def info(name):
+def info(name, path=None):
     a = (C.c_int * 6)()
-    if not lib().sqref_info(name.encode(), a):
+    if not lib(path).sqref_info(name.encode(), a):
         raise KeyError(name)
     return dict(L=a[0], D=a[1], weight=a[2], n=a[3], fixed=a[4], has_fv=bool(a[5]))
 
 
-def fd(name, sf, sqab=1):
+def fd(name, sf, sqab=1, path=None):
     sf = np.ascontiguousarray(sf, dtype=np.float64)
     f = np.empty(sf.shape[0]); ab = np.empty(sf.shape[0])
-    if not lib().sqref_fd(name.encode(), sf.shape[0], sf.ctypes.data, int(sqab), f.ctypes.data, ab.ctypes.data):
+    if not lib(path).sqref_fd(name.encode(), sf.shape[0], sf.ctypes.data, int(sqab), f.ctypes.data, ab.ctypes.data):
         raise KeyError(name)
     return f, ab
 
@@ -118,10 +120,10 @@ def fv(name, sf, sqab=1):
     return f, ab
 
 
-def fq(name, sf):
+def fq(name, sf, path=None):
     """double-double value and |.| sum as (n, 2) arrays of (hi, lo)"""
     sf = np.ascontiguousarray(sf, dtype=np.float64)
     f = np.empty((sf.shape[0], 2)); ab = np.empty((sf.shape[0], 2))
-    if not lib().sqref_fq(name.encode(), sf.shape[0], sf.ctypes.data, f.ctypes.data, ab.ctypes.data):
+    if not lib(path).sqref_fq(name.encode(), sf.shape[0], sf.ctypes.data, f.ctypes.data, ab.ctypes.data):
         raise KeyError(name)
     return f, ab

@@ -217,6 +217,13 @@ def count_flops(graphs):
         return json.load(f)
 
 
+def generate_only(kernels=DEFAULT_KERNELS, classes='pi6'):
+    """Run the code generator on classes that the library is not built with (default: pi6), so that their
+    generated headers can be checked on the host; returns the graph names (none without sources)."""
+    srcs = [f for f in kernel_sources(kernels, classes) if not f.startswith(SYNTH)]
+    return [g[0] for g in generate(srcs)] if srcs else []
+
+
 def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=True):
     """Generate and compile whatever is out of date; returns the library path."""
     srcs = kernel_sources(kernels, classes)

@@ -12,7 +12,7 @@ Fixtures
   boxsum_gl.json                the reference's pointwise known-answer program
                                 (mathematica/check/boxsum_gl.c): term values at k = 0 and k = (1,-1,2,0),
                                 h = 1, and full-box sums at h = 1, K = 6, for the five two-loop kernels
-  pointwise_<class>.npz         400 (g3: 128, v4/w4: 32) seeded nodes per graph, sigma = e^z, z ~ U[-3,3] (the protocol of
+  pointwise_<class>.npz         400 (g3: 128, v4/w4/pi6: 32) seeded nodes per graph, sigma = e^z, z ~ U[-3,3] (the protocol of
                                 tests/check_onept.sh): fd with SQ_AB = 1 and 0 and fq (hi, lo) of the
                                 reference kernels
   pointwise_synth.npz           the same for the synthetic integrands syn_d5, syn_d8, syn_d11 (64 nodes each),
@@ -85,17 +85,17 @@ def boxsum():
         json.dump(d, f, indent=1)
 
 
-def pointwise(cls, prefixes, npts=400):
+def pointwise(cls, prefixes, npts=400, path=None):
     rng = np.random.default_rng(12345)
     arrays = {}
-    for name in refpy.names():
+    for name in refpy.names(path):
         if not name.startswith(prefixes):
             continue
-        D = refpy.info(name)['D']
+        D = refpy.info(name, path)['D']
         sf = np.exp(rng.uniform(-3, 3, size=(npts, D)))
-        f1, a1 = refpy.fd(name, sf, 1)
-        f0, a0 = refpy.fd(name, sf, 0)
-        q, qa = refpy.fq(name, sf)
+        f1, a1 = refpy.fd(name, sf, 1, path)
+        f0, a0 = refpy.fd(name, sf, 0, path)
+        q, qa = refpy.fq(name, sf, path)
         arrays[name + '.sf'] = sf
         arrays[name + '.fd1'] = np.stack([f1, a1], 1)
         arrays[name + '.fd0'] = np.stack([f0, a0], 1)
@@ -199,6 +199,7 @@ if __name__ == '__main__':
         pointwise('g3', ('g3_',), 128)
         pointwise('v4', ('v4_',), 32)
         pointwise('w4', ('w4_',), 32)
+        pointwise('pi6', ('w4_p6',), 32, refpy.LIBSQREF_PI6)
     if 'synth' in parts:
         synth()
     if 'fold' in parts:

@@ -2,7 +2,9 @@
 graph, compiled for the host over double and over the double-double type of the device code
 (sincfeyn_b200/csrc/sqdd.cuh), without FP contraction, reproduces the reference kernels' values bit for
 bit at the seeded nodes of the golden fixtures (the double half f_d with SQ_AB = 1 and 0, and the
-double-double fq).  This is the same arithmetic the sm_100a build runs with -fmad=false."""
+double-double fq).  This is the same arithmetic the sm_100a build runs with -fmad=false.  The pi6 class,
+which the device library is not built with by default, is generated (build.generate_only) and checked
+here too."""
 import ctypes as C
 import os
 import subprocess
@@ -79,7 +81,7 @@ def class_lib(cls):
     return z, have, hostlib(have)
 
 
-@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3', 'v4', 'w4'])
+@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3', 'v4', 'w4', 'pi6'])
 def test_generated_kernels_match_the_reference_bitwise(cls):
     z, have, L = class_lib(cls)
     for n in have:
