@@ -5,33 +5,35 @@ fallback on the device.  Metric: integrand points per second and time-to-sum.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-A step is one integral's whole hierarchical sum through the public C ABI: the top-level grow and
-dilation, then every refinement level on the device.  K defaults to the whole set; the timed region is
-the K integrals as one concurrent batch (sqb_hsum_batch, worker count from the batch tuner), so its
-device time is the set's time-to-sum.  The same integrals then run one at a time, each kernel timed
-alone, for the level-pass throughput and the FP64 roofline.  The W warm-up steps run the first W
-integrals untimed, then the tuner runs every 4th integral once per candidate worker count.  With N ranks
-(torchrun) the integrals are dealt round-robin to the ranks (strong scaling, no collective on the data
-path); the time is the maximum over ranks.
+A step is the whole set: its 41 integrals as one concurrent batch through the public C ABI
+(sqb_hsum_batch: host parameters in, host results out; each integral's top-level grow and dilation, then
+every refinement level on the device; the worker count from the batch tuner, run once before the warm-up).
+W warm-up steps, then K timed steps; the step's device time is the set's time-to-sum.  The same integrals
+then run one at a time, each kernel timed alone, for the level-pass throughput and the FP64 roofline.
+With N ranks (torchrun) the integrals are dealt round-robin to the ranks (strong scaling, no collective on
+the data path); the time is the maximum over ranks.
 
 JSON line (rank 0):
   value      points/s of the device-resident refinement levels: evaluated children / device time of the
              level passes (cell lists already in HBM when each pass starts; CUDA events on the library's
-             stream)
-  e2e        points/s through sqb_hsum_batch with host-side parameters and host-side results, every
-             host<->device copy inside (all evaluated points / device time of the batch); time_to_sum_s
-             is that device time; one_at_a_time the same integrals through sqb_hsum one after another
+             stream), one integral at a time over the whole set
+  e2e        points/s of a step: all evaluated points of the set / device time of the batch, every
+             host<->device copy inside; ms_per_step and time_to_sum_s are that device time (mean of the K
+             steps); one_at_a_time the same integrals through sqb_hsum one after another
   roofline   the FP64 evaluation kernels (sqb_k_f64<graph>): algorithmic flops per point (+ - * / of the
              kernel's double path, counted by the code generator; skipped |.| sums counted as skipped) over
              their event-timed launches, against this device's FP64 FMA rate measured by a probe kernel
   cpu_baseline  the reference's own OpenMP CPU build (oracle/_ref/sincqed) on this host's cores, on a
-             bounded sample of the same workload
-  vs_alldd   a sample of the set (or the whole set, --alldd-full) in the contracted, the as-written and the
-             plain all-double-double forms, one integral at a time: time ratio
+             bounded sample of the same workload (integrals of D = 5, 5, 6, 7), with its rate per D
+  precision  the error of the results: a sample's FP64 + dd values against all-double-double GPU runs of
+             the same integrals (two D = 7 graphs; --alldd-full: the whole set) with both forms' times, the
+             set sum against the analytic A1^(6), and every integral against the reference CPU run of the
+             workload (the committed fixture tests/golden/all3_h0.7_N139_eps1e-12.json)
   fold       the same batch with the symmetry fold (sym='auto': each integrand's group of axis
              permutations, as the reference CPU build finds it): time-to-sum, evaluated points, the largest
              relative difference from the unfolded values, the group orders
-`--impl reference` times the reference CPU build on the same metric (rank 0 only).
+`--impl reference` times the reference CPU build on the same metric (rank 0 only), one integral of the CPU
+sample per step.
 
 Other measurements (one GPU, each prints its own JSON lines; not the headline):
   --workload mixed   all2 + all3 at h = 1.0, 0.9, 0.8, 0.7 (184 integrals): one at a time against the
@@ -59,9 +61,11 @@ sys.path.insert(0, ROOT)
 
 H, N_PTS, EPS = 0.7, 139, 1e-12
 SET = 'all3'
-# the CPU samples: three-loop integrals of D = 5, 5 and 6 at the workload's (h, N, eps)
-CPU_SAMPLE = ['g3_07', 'v3_01', 'g3_01']
-ALLDD_SAMPLE = ['v3_01', 'g3_07', 'g3_01', 'g3_00']
+# the CPU sample: three-loop integrals of D = 5, 5, 6 and 7 at the workload's (h, N, eps); by points it is
+# mostly D = 7, as the set is (13 of its 41 integrals, about nine tenths of its points)
+CPU_SAMPLE = ['g3_07', 'v3_01', 'g3_01', 'g3_00']
+# the precision sample: FP64 + dd against all-dd, two D = 7 graphs among them
+ALLDD_SAMPLE = ['v3_01', 'g3_07', 'g3_01', 'g3_00', 'g3_12']
 PROFILE_TRAFFIC = os.path.join(ROOT, 'profiles', 'fp64_kernel_traffic.json')
 BATCH_CANDIDATES = (2, 4, 8)     # worker streams tried by the batch tuner
 
@@ -124,9 +128,9 @@ class Clocks:
                 'reasons': sorted(reasons)}
 
 
-def cpu_reference(graphs, threads, budget_s=None):
-    """The reference CPU build (oracle/_ref/sincqed, symmetry fold on as shipped) on these integrals;
-    returns (evals, seconds, per-graph rows)."""
+def cpu_reference(graphs, threads):
+    """The reference CPU build (oracle/_ref/sincqed, symmetry fold on as shipped) on these integrals, one
+    process each; returns (evals, seconds, per-graph rows)."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     import refpy
     if not refpy.available():
@@ -139,29 +143,31 @@ def cpu_reference(graphs, threads, budget_s=None):
         ev += r[0]['evals']
         sec += dt
         rows.append({'graph': g, 'evals': r[0]['evals'], 'seconds': round(dt, 3), 'value': r[0]['value']})
-        if budget_s and sec > budget_s:
-            break
     return ev, sec, rows
 
 
 def run_reference(args, rank):
-    """--impl reference: the reference's CPU implementation of the path, all host threads, one integral of
-    the CPU sample per step (cycling), same metric."""
+    """--impl reference: the reference's CPU implementation of the path (oracle/_ref/sincqed, its OpenMP build,
+    all host threads), same metric.  A step of ours is the whole set (minutes of CPU time per integral of
+    D = 7, an hour or more for the set); a step here is one integral of the CPU sample in turn, which keeps
+    the run to minutes: the warm-up steps run its cheapest integral."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    seq = [CPU_SAMPLE[i % len(CPU_SAMPLE)] for i in range(args.warmup + args.steps)]
-    cpu_reference(seq[:args.warmup], threads)
-    ev, sec, rows = cpu_reference(seq[args.warmup:], threads)
+    seq = [CPU_SAMPLE[i % len(CPU_SAMPLE)] for i in range(args.steps)]
+    cpu_reference([CPU_SAMPLE[0]]*args.warmup, threads)
+    ev, sec, rows = cpu_reference(seq, threads)
     v = ev/sec
     line = {'impl': 'reference', 'metric': 'integrand points/s (time-to-sum) of the three-loop set at h=0.7',
             'value': v, 'unit': 'points/s', 'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': 1e3*sec/args.steps, 'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None,
             'dtype': 'f64+dd', 'data': 'the reference kernels (kernels/g3, kernels/v3), no external data',
-            'config': {'workload': 'all3 sample %s at h=%g N=%d eps=%g' % (','.join(CPU_SAMPLE), H, N_PTS, EPS),
+            'config': {'workload': 'all3 at h=%g N=%d eps=%g: a sample, one integral per step cycling over %s (D = 5, 5, 6, 7)'
+                                   % (H, N_PTS, EPS, ','.join(CPU_SAMPLE)),
                        'cpu': 'oracle/_ref/sincqed (reference CPU build, OpenMP)'},
             'cpu_baseline': {'value': v, 'unit': 'points/s', 'cores': threads, 'kind': 'reference',
-                             'sample': '%d integrals cycling over %s' % (args.steps, ','.join(CPU_SAMPLE))},
+                             'sample': '%d integrals cycling over %s' % (args.steps, ','.join(CPU_SAMPLE)),
+                             'rows': rows},
             'e2e': {'value': v, 'unit': 'points/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
 
@@ -359,12 +365,12 @@ def run_synth(args, sq, L):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=None, help='integrals timed (default: the whole set)')
-    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--steps', type=int, default=3, help='timed steps, each the whole set as one batch')
+    ap.add_argument('--warmup', type=int, default=3, help='untimed steps before them (at least 3)')
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-alldd', action='store_true', help='skip the all-double-double comparison')
-    ap.add_argument('--alldd-full', action='store_true', help='all-double-double comparison on the whole set (~2 min)')
+    ap.add_argument('--alldd-full', action='store_true', help='all-double-double comparison on the whole set (~6 min)')
     ap.add_argument('--no-fold', action='store_true', help='skip the batch with the symmetry fold')
     ap.add_argument('--fold', action='store_true', help='--workload vp4: with the symmetry fold (sym=auto)')
     ap.add_argument('--predict', type=float, default=0.0, help='--workload vp4: the last-level predictor with this alpha')
@@ -378,6 +384,7 @@ def main():
                          'synth: the synthetic microbenchmark and its precision table; vp4: the four-loop '
                          'lepton-loop set at h=1.0 and 0.9 (one GPU)')
     args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
     rank, world, local = env_rank()
     if args.workload != 'all3':
         if rank == 0 and args.impl == 'ours':
@@ -394,8 +401,6 @@ def main():
         import datetime
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
     if args.impl == 'reference':
-        if args.steps is None:
-            args.steps = 41
         run_reference(args, rank)
         if world > 1:
             import torch.distributed as dist
@@ -405,13 +410,9 @@ def main():
     import torch
     from sincfeyn_b200 import sq
     torch.cuda.set_device(local)
-    o = sq.default_opts(device=local)
     names = sq.select([SET])
-    if args.steps is None:
-        args.steps = len(names)
-    order = [names[i % len(names)] for i in range(args.steps)]
     D_OF = {x['name']: x['D'] for x in sq.graphs()}
-    mine = assign(order, rank, world)
+    mine = assign(names, rank, world)
     L = sq.lib()
     import ctypes as C
     L.sqb_timer_stop.restype = C.c_double
@@ -425,16 +426,15 @@ def main():
     for g in names:
         sq.preload(g)
     t_load = time.perf_counter() - t_load
-    # warm-up: the first W integrals of the set, untimed; then the batch tuner on every 4th integral of
-    # this rank's share (it also warms the worker threads' buffers)
-    for g in names[:args.warmup]:
-        sq.hsum(g, H, N_PTS, EPS, device=local)
     # cost estimate for the largest-first order: children per cell times flops per point
     jobs = [(g, H, N_PTS, EPS, -1, float(2**D_OF[g])*sq.flops(g, 1)) for g in mine]
-    # the tuning sample leaves out the costliest integral: alone it sets the sample's time whatever the
-    # worker count, which would make the choice noise
+    # the batch tuner (untimed): every 4th integral of this rank's share once per candidate worker count;
+    # the sample leaves out the costliest integral, which alone would set its time whatever the count
     top = max(j[5] for j in jobs)
     workers, tune_rates = sq.batch_tune([j for j in jobs if j[5] < top][::4], BATCH_CANDIDATES, device=local)
+    # W warm-up steps: the whole share as one batch, untimed
+    for _ in range(args.warmup):
+        sq.hsum_batch(jobs, workers=workers, device=local)
     peak = sq.probe_fp64(True)
     flops = {g: (sq.flops(g, 1), sq.flops(g, 0)) for g in names}
     weight = {x['name']: x['weight'] for x in sq.graphs()}
@@ -445,39 +445,50 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
-    # the timed region: this rank's integrals as one concurrent batch (sqb_hsum_batch), device time
-    L.sqb_l2_flush(256 << 20)
-    t_wall = time.perf_counter()
-    bres, batch_ms = sq.hsum_batch(jobs, workers=workers, device=local)
-    wall = time.perf_counter() - t_wall
+    # the timed region: K steps, each this rank's whole share of the set as one concurrent batch through
+    # the C ABI (sqb_hsum_batch: host parameters in, host results out), its device time by CUDA events;
+    # L2 flushed before every step
+    step_ms, walls, bres, same_steps = [], [], None, True
+    for _ in range(args.steps):
+        L.sqb_l2_flush(256 << 20)
+        t_wall = time.perf_counter()
+        res, ms = sq.hsum_batch(jobs, workers=workers, device=local)
+        walls.append(time.perf_counter() - t_wall)
+        step_ms.append(ms)
+        if bres is None:
+            bres = res
+        else:
+            same_steps = same_steps and all(_same(a['S'][0], b['S'][0]) and a['nev'] == b['nev'] for a, b in zip(res, bres))
+    torch.cuda.synchronize()
+    clk = clocks.stop()
     h1 = (C.c_ulonglong(), C.c_ulonglong())
     L.sqb_copy_bytes(C.byref(h1[0]), C.byref(h1[1]))
     nev = sum(r['nev'] for r in bres)
-    launches = sum(r['launches'] for r in bres)
+    launches = sum(r['launches'] for r in bres)*args.steps
     bvals = {j[0]: r['S'][0] for j, r in zip(jobs, bres)}
     # the same integrals one at a time, each kernel timed alone: the level-pass throughput and the FP64
     # roofline (a kernel that shares the device with other streams would read slow)
     sq.kernel_timing(True)
-    step_ms, lev_ms, lev_ev, f64_ms, f64_n, fl, results, same = 0.0, 0.0, 0, 0.0, 0, 0.0, [], True
+    one_ms, lev_ms, lev_ev, f64_ms, f64_n, fl, results, same = 0.0, 0.0, 0, 0.0, 0, 0.0, [], True
     for g in mine:
         L.sqb_l2_flush(256 << 20)
         L.sqb_timer_start()
         r = sq.hsum(g, H, N_PTS, EPS, device=local)
         ms = L.sqb_timer_stop()
-        step_ms += ms
+        one_ms += ms
         lev_ms += sum(r['lev_ms'])
         lev_ev += sum(r['lev_evals'])
         f64_ms += r['f64_ms']
         f64_n += r['f64_launches']
         a1, a0 = flops[g]
         fl += (r['nev'] - r['abskipped'])*a1 + r['abskipped']*a0
-        same = same and (r['S'][0] == bvals[g] or (r['S'][0] != r['S'][0] and bvals[g] != bvals[g]))
-        results.append([g, r['S'][0]*weight[g], r['nev'], r['nq'], round(ms, 2), round(1e3*r['t_top'], 2),
+        same = same and _same(r['S'][0], bvals[g])
+        results.append([g, D_OF[g], r['S'][0]*weight[g], r['nev'], r['nq'], round(ms, 2), round(1e3*r['t_top'], 2),
                         round(sum(r['lev_ms']), 2)])
+    sq.kernel_timing(False)
     # the same batch with the symmetry fold (sym='auto', the reference CPU build's default): the same kept
     # tree and values to rounding, fewer evaluations; reported beside the headline, not in it
     fold_ms, fnev, fdiff, groups, fold_err = 0.0, 0, 0.0, {}, None
-    sq.kernel_timing(False)
     if not args.no_fold:
         try:
             L.sqb_l2_flush(256 << 20)
@@ -490,11 +501,12 @@ def main():
         except sq.SqbError as e:                   # reported beside the headline, which stands without it
             fold_ms, fold_err = 0.0, str(e)[:200]
     torch.cuda.synchronize()
-    clk = clocks.stop()
-    mx, sm = reduce_max_sum([batch_ms, step_ms, wall, fold_ms, fdiff],
+    batch_ms = statistics.mean(step_ms)
+    wall = statistics.mean(walls)
+    mx, sm = reduce_max_sum([batch_ms, min(step_ms), max(step_ms), one_ms, wall, fold_ms, fdiff],
                             [lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches, h1[0].value - h0[0].value,
-                             h1[1].value - h0[1].value, 0 if same else 1, fnev], world)
-    batch_ms, step_ms, wall, fold_ms, fdiff = mx
+                             h1[1].value - h0[1].value, 0 if same and same_steps else 1, fnev], world)
+    batch_ms, step_min, step_max, one_ms, wall, fold_ms, fdiff = mx
     lev_ms, lev_ev, nev, f64_ms, f64_n, fl, launches, h2d, d2h, ndiff, fnev = sm
     if rank != 0:
         if world > 1:
@@ -511,22 +523,24 @@ def main():
     line = {
         'metric': 'integrand points/s (time-to-sum) of the three-loop set at h=0.7',
         'value': lev_ev/(lev_ms*1e-3) if lev_ms > 0 else None, 'unit': 'points/s',
-        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': batch_ms/max(1, len(mine)),
+        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': batch_ms,
         'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f64+dd',
         'data': 'the reference kernels (kernels/g3, kernels/v3) as integrands; no external data',
-        'precision': 'FP64 pass contracted (fused multiply-adds), double-double fallback and level sums',
+        'precision_form': 'FP64 pass contracted (fused multiply-adds), double-double fallback and level sums',
         'config': {'workload': '%s (%d integrals) h=%g N=%d eps=%g top=2, FP64 + double-double fallback'
                                % (SET, len(names), H, N_PTS, EPS),
-                   'integrals_timed': args.steps,
-                   'l2': 'flushed (256 MiB memset) before the batch and before every one-at-a-time integral',
+                   'step': 'the whole set (all %d integrals) as one concurrent batch through sqb_hsum_batch' % len(names),
+                   'l2': 'flushed (256 MiB memset) before every step and before every one-at-a-time integral',
                    'kernels': 'device code of the set\'s kernels loaded before the timed region (load_s %.2f s, once per process)' % t_load,
                    'parallelism': 'integrals dealt round-robin over %d GPU(s); on each, one concurrent batch of %d worker streams'
                                   % (world, workers)},
-        'time_to_sum_s': batch_ms*1e-3 if args.steps >= len(names) else None,
+        'time_to_sum_s': batch_ms*1e-3,
+        'time_to_sum_steps_s': {'mean': batch_ms*1e-3, 'min': step_min*1e-3, 'max': step_max*1e-3},
         'e2e': {'value': nev/(batch_ms*1e-3), 'unit': 'points/s', 'h2d_bytes_per_step': int(h2d/args.steps),
-                'd2h_bytes_per_step': int(d2h/args.steps), 'wall_s': wall},
+                'd2h_bytes_per_step': int(d2h/args.steps), 'wall_s_per_step': wall,
+                'note': 'the whole set per step through the C ABI (host parameters in, host results out)'},
         'batch': {'workers': workers, 'tuner_points_s': tune_rates, 'device_s': batch_ms*1e-3},
-        'one_at_a_time': {'device_s': step_ms*1e-3, 'points_s': nev/(step_ms*1e-3),
+        'one_at_a_time': {'device_s': one_ms*1e-3, 'points_s': nev/(one_ms*1e-3),
                           'same_values_as_batch': ndiff == 0},
         'fold': None if args.no_fold else {'unavailable': fold_err} if fold_err or not fold_ms else {
             'time_to_sum_s': fold_ms*1e-3, 'points': int(fnev), 'speedup_vs_unfolded': batch_ms/fold_ms,
@@ -543,35 +557,89 @@ def main():
         'clocks': clk,
         'points': int(nev), 'level_points': int(lev_ev),
     }
+    if world == 1:
+        line['precision'] = precision_table(args, sq, L, names, {g: v*weight[g] for g, v in bvals.items()}, line)
     if world == 1 and not args.no_cpu:
         try:
-            ev, sec, rows = cpu_reference(CPU_SAMPLE, os.cpu_count() or 1, budget_s=30)
+            ev, sec, rows = cpu_reference(CPU_SAMPLE, os.cpu_count() or 1)
+            per_d = {}
+            for r in rows:
+                x = per_d.setdefault(D_OF[r['graph']], [0, 0.0])
+                x[0] += r['evals']
+                x[1] += r['seconds']
             line['cpu_baseline'] = {'value': ev/sec, 'unit': 'points/s', 'cores': os.cpu_count() or 1, 'kind': 'reference',
-                                    'sample': 'reference CPU build on %s at h=%g N=%d eps=%g (%.1f s)'
-                                              % (','.join(r['graph'] for r in rows), H, N_PTS, EPS, sec)}
+                                    'sample': 'reference CPU build (OpenMP, all host threads) on %s (D = %s) at h=%g N=%d '
+                                              'eps=%g, one integral at a time (%.1f s)'
+                                              % (','.join(r['graph'] for r in rows),
+                                                 ','.join(str(D_OF[r['graph']]) for r in rows), H, N_PTS, EPS, sec),
+                                    'points_s_by_D': {str(d): v[0]/v[1] for d, v in sorted(per_d.items())},
+                                    'rows': rows}
         except Exception as e:                      # the oracle binary is test infrastructure; report why
             line['cpu_baseline'] = {'value': None, 'unavailable': str(e)[:200]}
-    if world == 1 and not args.no_alldd:
-        sample = names if args.alldd_full else ALLDD_SAMPLE
-        t = {}
+    line['per_integral'] = {'columns': ['graph', 'D', 'value', 'evals', 'fallback', 'ms', 'top_ms', 'levels_ms'],
+                            'rows': results}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def _same(a, b):
+    return a == b or (a != a and b != b)
+
+
+A1_6 = 1.181241456587          # the analytic three-loop coefficient (docs/REPRODUCE.md:98-100)
+GOLDEN_ALL3 = os.path.join(ROOT, 'tests', 'golden', 'all3_h0.7_N139_eps1e-12.json')
+
+
+def precision_table(args, sq, L, names, values, line):
+    """The error of the results: per integral of a sample (two D = 7 graphs among them; --alldd-full: the whole
+    set) the FP64 + double-double value against the all-double-double GPU run of the same integral, with
+    both forms' times; the set's sum against the analytic A1^(6); and, where the reference CPU run of the
+    workload is among the committed fixtures, every integral against it."""
+    out = {'form': line['precision_form']}
+    sample = names if args.alldd_full else ALLDD_SAMPLE
+    if not args.no_alldd:
+        t, vals = {}, {}
         try:
             for form, kw in (('fp64dd', {}), ('fp64dd_as_written', {'fma': 0}), ('alldd', {'alldd': 1})):
                 sq.hsum(sample[0], H, N_PTS, EPS, **kw)                 # warm: this form's kernels and buffers
                 t[form] = 0.0
                 for g in sample:
                     L.sqb_l2_flush(256 << 20)
-                    L.sqb_timer_start(); sq.hsum(g, H, N_PTS, EPS, **kw); t[form] += L.sqb_timer_stop()*1e-3
-            line['vs_alldd'] = {'sample': 'all %d integrals' % len(sample) if args.alldd_full else sample,
-                                'fp64dd_s': t['fp64dd'], 'fp64dd_as_written_s': t['fp64dd_as_written'],
-                                'alldd_s': t['alldd'], 'speedup': t['alldd']/t['fp64dd'],
-                                'note': 'one integral at a time, each form warmed first, L2 flushed before each integral'}
+                    L.sqb_timer_start()
+                    r = sq.hsum(g, H, N_PTS, EPS, **kw)
+                    t[form] += L.sqb_timer_stop()*1e-3
+                    vals.setdefault(g, {})[form] = r['S'][0]
+            rel = {g: abs(v['fp64dd'] - v['alldd'])/abs(v['alldd']) for g, v in vals.items()}
+            rel_w = {g: abs(v['fp64dd_as_written'] - v['alldd'])/abs(v['alldd']) for g, v in vals.items()}
+            out['vs_alldd'] = {'sample': 'all %d integrals' % len(sample) if args.alldd_full else sample,
+                               'rel_err_fp64dd': rel, 'rel_err_fp64dd_as_written': rel_w,
+                               'max_rel_err': max(rel.values()), 'fp64dd_s': t['fp64dd'],
+                               'fp64dd_as_written_s': t['fp64dd_as_written'], 'alldd_s': t['alldd'],
+                               'speedup': t['alldd']/t['fp64dd'],
+                               'note': 'one integral at a time, each form warmed first, L2 flushed before each integral'}
+            line['vs_alldd'] = {'sample': out['vs_alldd']['sample'], 'speedup': t['alldd']/t['fp64dd'],
+                                'fp64dd_s': t['fp64dd'], 'alldd_s': t['alldd']}
         except sq.SqbError as e:                   # reported beside the headline, which stands without it
-            line['vs_alldd'] = {'unavailable': str(e)[:200]}
-    line['per_integral'] = {'columns': ['graph', 'value', 'evals', 'fallback', 'ms', 'top_ms', 'levels_ms'], 'rows': results}
-    print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+            out['vs_alldd'] = {'unavailable': str(e)[:200]}
+    total = sum(values.values())
+    out['set_sum'] = {'value': total, 'A1_6': A1_6, 'diff': total - A1_6,
+                      'note': 'the sum of weight x value over the 41 integrals; the Sinc sum at h=0.7 with top=2 '
+                              'differs from the analytic value by its discretisation and pruning errors'}
+    if os.path.exists(GOLDEN_ALL3):
+        with open(GOLDEN_ALL3) as f:
+            gold = {r['name']: r for r in json.load(f)['rows']}
+        common = [g for g in names if g in gold and g in values]
+        if common:
+            rel = {g: abs(values[g] - gold[g]['value'])/abs(gold[g]['value']) for g in common}
+            worst = max(rel, key=rel.get)
+            ref_sum = sum(gold[g]['value'] for g in common)
+            out['vs_reference_cpu'] = {'integrals': len(common), 'max_rel': rel[worst], 'worst': worst,
+                                       'reference_set_sum': ref_sum if len(common) == len(names) else None,
+                                       'source': 'tests/golden/all3_h0.7_N139_eps1e-12.json (sincqed-exact, SINCQED_SYM=0, '
+                                                 'SINCQED_KEEPBT=1)'}
+    return out
 
 
 if __name__ == '__main__':

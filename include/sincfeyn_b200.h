@@ -44,6 +44,13 @@ void gpu_wait(int slot, const double **fw, const double **abw);
 void gpu_submit_cells(int slot, long nc, const int *cells, int stride, const unsigned char *skip, int st);
 /* driver/gpu.h:28 */
 const char *gpu_info(void);
+/* The plug-in launcher of GG_<graph> (sq_gpu_launch_t, same arguments and device buffers) with the build
+ * chosen: form 0 = the FP64 kernel rounded as written (what GG_<graph> runs), 2 = the contracted FP64
+ * kernel (fused multiply-adds).  Not in the reference's ABI: it lets a caller, or a benchmark that times
+ * the reference's own plug-in kernel, run either build on the same nodes.  0, or -1 (no such graph or
+ * build; sqb_error() has the message) */
+int  sqb_plugin_launch(const char *graph, int form, sq_stream_t st, long n, const short *k, const unsigned char *skip,
+                       const double *EX, int K, double H, double *of, double *oab, int cmode, int cst);
 
 /* ------------------------------------------------------------------------------------------------
  * 2. Chosen form
@@ -231,7 +238,11 @@ int  sqb_l2_flush(size_t bytes);
  *      kept children that did not fit next_cap;
  *    - at most SQB_NOALLOC_CHILDREN children (ncell << D) per call, else SQB_NOALLOC_TOO_BIG and nothing
  *      runs; calls share the scratch, so calls whose GPU work overlaps race: issue them one at a time;
- *      the first call on a device looks up the scratch address, so make it before any stream capture.
+ *      the first call on a device looks up the scratch address, so make it before any stream capture;
+ *    - each call waits for its stream before it returns (the sums and counters are host arrays): the host
+ *      blocks until the call's GPU work is done;
+ *    - the scratch is SQB_NOALLOC_BYTES of device memory on every GPU that loads the library, held until
+ *      the process exits (the layout is checked against this size when the library is compiled).
  *    Returns 0, a negative SQB_NOALLOC_* code or a CUDA error code; sqb_error() has the message. */
 #define SQB_NOALLOC_CHILDREN (1L << 18)
 #define SQB_NOALLOC_BYTES (6700000L)

@@ -1,9 +1,9 @@
 """Build of the evaluator: generated per-graph CUDA, the runtime, the C-ABI library and the CLI.
 
-    python -m sincfeyn_b200.build [--kernels DIR] [--classes "g2 g3 v3"] [-j N]
+    python -m sincfeyn_b200.build --kernels DIR [--classes "g2 g3 v3"] [-j N]
 
 Inputs are the generated sincFeyn kernel sources (kernels/<class>/<g>.c of the reference tree, the same
-files its tools/gpugen.py reads).  Outputs, all in-tree and git-ignored:
+files its tools/gpugen.py reads): DIR is that kernels/ directory, given by --kernels or SQB_KERNELS.  Outputs, all in-tree and git-ignored:
   sincfeyn_b200/_build/gen/   kgen output (<g>.cuh), the per-graph translation units, the registry;
   sincfeyn_b200/_build/obj/   objects;
   sincfeyn_b200/lib/libsqb200.so   the C ABI (include/sincfeyn_b200.h), every graph's sm_100a kernels;
@@ -32,7 +32,7 @@ OBJ = os.path.join(BUILD, 'obj')
 LIB = os.path.join(PKG, 'lib')
 BIN = os.path.join(PKG, 'bin')
 INC = os.path.join(ROOT, 'include')
-DEFAULT_KERNELS = os.environ.get('SQB_KERNELS', '/root/reference/kernels')
+DEFAULT_KERNELS = os.environ.get('SQB_KERNELS')     # the reference's kernels/ directory (no default)
 DEFAULT_CLASSES = os.environ.get('SQB_CLASSES', 'g2 g3 v3 v4 w4')
 
 NVCC = os.environ.get('NVCC', 'nvcc')
@@ -56,6 +56,22 @@ def _newer(out, ins):
         return True
     t = os.path.getmtime(out)
     return any(os.path.getmtime(i) > t for i in ins if os.path.exists(i))
+
+
+def _flags_stamp():
+    """A file holding the contracted units' compile policy (flags, spill limit, occupancy candidates): an
+    input of every such unit, rewritten -- so newer than the objects -- only when the policy changes.  A
+    first stamp is dated to the epoch: objects already built are taken to follow the policy."""
+    path = os.path.join(BUILD, 'fma_policy.txt')
+    text = json.dumps({'flags': NVFLAGS_FMA, 'spill_max': SPILL_MAX}) + '\n'
+    old = open(path).read() if os.path.exists(path) else None
+    if old != text:
+        os.makedirs(BUILD, exist_ok=True)
+        with open(path, 'w') as f:
+            f.write(text)
+        if old is None:
+            os.utime(path, (0, 0))
+    return path
 
 
 def _run(cmd, log=None):
@@ -107,6 +123,8 @@ def _compile_graph(tu, o, tuf, of, name, do_exact, do_fma):
 def kernel_sources(kdir, classes):
     """the reference's kernels of these classes, then the synthetic integrands of sincfeyn_b200/synth"""
     out = []
+    if not kdir:
+        return out
     for c in classes.split():
         d = os.path.join(kdir, c)
         if os.path.isdir(d):
@@ -126,9 +144,12 @@ def generate(srcs):
         base = os.path.splitext(os.path.basename(src))[0]
         cuh = os.path.join(GEN, base + '.cuh')
         if _newer(cuh, [src] + me):
+            # rewritten only when the text changes, so that a generator change that leaves a graph's
+            # output as it was does not recompile that graph
             k, text = kgen.emit(src)
-            with open(cuh, 'w') as f:
-                f.write(text)
+            if not os.path.exists(cuh) or open(cuh).read() != text:
+                with open(cuh, 'w') as f:
+                    f.write(text)
         with open(cuh) as f:
             m = re.search(r'^SQ_GRAPH(?:_SPLIT)?\((\w+), "((?:[^"\\]|\\.)*)", (\d+), (\d+),', f.read(), re.M)
         name, D = m.group(1), int(m.group(4))
@@ -230,7 +251,8 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     if not srcs:
         if os.path.exists(LIBSO):
             return LIBSO
-        raise RuntimeError('no kernel sources under %s and no prebuilt %s' % (kernels, LIBSO))
+        raise RuntimeError('no kernel sources under %s and no prebuilt %s: give the reference\'s kernels/ '
+                           'directory (--kernels DIR or SQB_KERNELS)' % (kernels, LIBSO))
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIB, exist_ok=True)
     os.makedirs(BIN, exist_ok=True)
@@ -240,12 +262,13 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
     hdrs = [os.path.join(CSRC, f) for f in ('sqkern.cuh', 'sqdd.cuh', 'sqscale.cuh', 'sqorbit.cuh', 'sqb_internal.h', 'sqb_rt.h')] + \
            [os.path.join(INC, 'sincfeyn_b200.h')]
     khdrs = [os.path.join(CSRC, f) for f in ('sqkern.cuh', 'sqdd.cuh', 'sqscale.cuh', 'sqorbit.cuh', 'sqb_internal.h')]   # what a graph TU includes
+    stamp = _flags_stamp()
     jobs_list = []
     for name, D, cuh, tu in graphs:
         o = os.path.join(OBJ, 'k_%s.o' % name)
         of = os.path.join(OBJ, 'kf_%s.o' % name)
         tuf = os.path.join(GEN, 'kf_%s.cu' % name)
-        do_fma = _newer(of, [tuf, cuh] + khdrs + [os.path.abspath(__file__)])
+        do_fma = _newer(of, [tuf, cuh, stamp] + khdrs)
         do_exact = do_fma or _newer(o, [tu, cuh] + khdrs)
         if do_fma or do_exact:
             jobs_list.append(lambda a=(tu, o, tuf, of, name, do_exact, do_fma): _compile_graph(*a))

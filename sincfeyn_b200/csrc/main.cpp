@@ -47,55 +47,6 @@ static int selected(const char *name, const char *volkov, int L, const char *s){
 }
 static int isnum(const char *s){ char *e; strtod(s, &e); return e != s && *e == 0; }
 
-/* `sincqed compare R1 R2` (driver/main.c:116-150): the per-graph error of a run at step h from a second
- * run at a larger step h' (about 1.2 h), |S(h) - S(h')|/3 + round, from two results files.  A results
- * line's value column is its first signed number of 20 or more characters with an exponent; h sits four
- * columns before it and the round column five after; a later line of the same graph replaces an earlier
- * one. */
-struct CompareRow { std::string name; double h, v, rnd; };
-static int read_results(const char *fn, std::vector<CompareRow> &rows){
-    FILE *f = fopen(fn, "r");
-    if(!f){ perror(fn); return -1; }
-    char line[4096];
-    while(fgets(line, sizeof line, f)){
-        if(line[0] == '#') continue;
-        std::vector<char*> tok;
-        for(char *t = strtok(line, " \t\n"); t && tok.size() < 64; t = strtok(NULL, " \t\n")) tok.push_back(t);
-        const int nt = (int)tok.size();
-        int iv = -1;
-        for(int i = 1; i < nt && iv < 0; i++)
-            if((tok[i][0] == '+' || tok[i][0] == '-') && strlen(tok[i]) >= 20 && strchr(tok[i], 'e')) iv = i;
-        if(iv < 5 || iv + 5 >= nt) continue;
-        size_t j = 0;
-        while(j < rows.size() && rows[j].name != tok[0]) j++;
-        if(j == rows.size()){ if(rows.size() == 2048) continue; rows.push_back(CompareRow()); }
-        rows[j].name = std::string(tok[0]).substr(0, 31);
-        rows[j].h = atof(tok[iv - 4]); rows[j].v = atof(tok[iv]); rows[j].rnd = atof(tok[iv + 5]);
-    }
-    fclose(f);
-    return 0;
-}
-static int compare(const char *fa, const char *fb){
-    std::vector<CompareRow> A, B;
-    if(read_results(fa, A) || read_results(fb, B)) return 1;
-    printf("# compare %s and %s: value from the smaller step h; error = |S(h) - S(h')|/3 + round\n", fa, fb);
-    printf("# (calibrated on graph 16, LbL and the Pi2 Pi2 chain with h = 1.0, h' = 1.2: true error <= |dS|/3)\n");
-    printf("# %-8s %6s %6s  %22s  %10s  %10s\n", "name", "h", "h'", "value", "dS", "error");
-    double tot = 0, e1 = 0, e2 = 0; int m = 0;
-    for(const CompareRow &a : A)
-        for(const CompareRow &b : B){
-            if(a.name != b.name) continue;
-            const CompareRow &fine = a.h <= b.h ? a : b, &coarse = a.h <= b.h ? b : a;
-            if(fine.h == coarse.h){ printf("  %-8s same h in both files, skipped\n", fine.name.c_str()); break; }
-            const double d = fine.v - coarse.v, e = fabs(d)/3 + fine.rnd;
-            printf("  %-8s %6.3f %6.3f  %+22.15e  %+10.2e  %10.2e\n", fine.name.c_str(), fine.h, coarse.h, fine.v, d, e);
-            tot += fine.v; e1 += e; e2 += e*e; m++;
-            break;
-        }
-    printf("# SUM %d graphs  %+.12f  err %.2e (in quadrature)  %.2e (linear)\n", m, tot, sqrt(e2), e1);
-    return 0;
-}
-
 static FILE *LOGF, *RESF;
 static void say(const char *fmt, ...){
     va_list ap; va_start(ap, fmt); vprintf(fmt, ap); va_end(ap); fflush(stdout);
@@ -129,12 +80,8 @@ int main(int argc, char **argv){
         printf("%d graphs (one per mirror pair; w = mirror weight), precision fallback double-double on the GPU\n", NG);
         for(int i = 0; i < NG; i++){ int info[6]; const char *n = sqb_graph_name(i); sqb_graph_info(n, info);
             printf("  %-8s L=%d  %-22s D=%d w=%d\n", n, info[0], sqb_graph_volkov(n), info[1], info[2]); }
-        printf("usage: %s run h N [eps] [top] GRAPH... | scale GRAPH [kappa] [seed] | compare R1 R2\n", argv[0]);
+        printf("usage: %s run h N [eps] [top] GRAPH... | scale GRAPH [kappa] [seed]\n", argv[0]);
         return 0;
-    }
-    if(!strcmp(argv[1], "compare")){
-        if(argc < 4){ fprintf(stderr, "compare RESULTS_h RESULTS_h2   (two results files, e.g. h = 1.0 and 1.2)\n"); return 1; }
-        return compare(argv[2], argv[3]);
     }
     /* the scaling test (driver/main.c:192-199), on the device */
     if(!strcmp(argv[1], "scale")){

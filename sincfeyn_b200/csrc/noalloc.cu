@@ -19,7 +19,10 @@
  *   - calls whose GPU work overlaps (two host threads, or two streams, on one device) race on the array:
  *     issue them one after another;
  *   - the first call on each device looks up the array's device address (cudaGetSymbolAddress) with that
- *     device current; make that first call before any stream capture.
+ *     device current; make that first call before any stream capture;
+ *   - every call copies the lattice tables from host memory and waits for its stream before it returns
+ *     (the sums and counters come back to the caller's host arrays): the host blocks until the call's
+ *     GPU work is done.
  * No cudaMalloc, cudaFree or allocating library routine is called. */
 #include <cuda_runtime.h>
 #include <math.h>
@@ -29,27 +32,33 @@
 #include "sincfeyn_b200.h"
 
 #define NA_CH SQB_NOALLOC_CHILDREN
-#define NA_TILES ((NA_CH + 2047)/2048 + 1)
-/* layout of the scratch array (offsets in bytes, each 256-aligned) */
-#define NA_TAB   0                                   /* X[255], Wt[255] */
-#define NA_V     (NA_TAB + 4096)                     /* double v[NA_CH] */
+/* tiles of the level tail (sqb_level_tail: SQB_TILE children each), one spare */
+#define NA_TILES ((NA_CH + SQB_TILE - 1)/SQB_TILE + 1)
+#define NA_UP(x) ((((long)(x)) + 255)/256*256)
+/* layout of the scratch array: offsets in bytes, each a multiple of 256 */
+#define NA_TAB   0L                                  /* X[255], Wt[255] */
+#define NA_V     (NA_TAB + 4096L)                    /* double v[NA_CH] */
 #define NA_UU    (NA_V + 8L*NA_CH)                   /* double uu[NA_CH] */
 #define NA_FB    (NA_UU + 8L*NA_CH)                  /* long fb[NA_CH] */
 #define NA_STT   (NA_FB + 8L*NA_CH)                  /* unsigned char stt[NA_CH] */
-#define NA_BP    (NA_STT + ((NA_CH + 255)/256)*256L)  /* tile partials */
-#define NA_BK    (NA_BP + 128L*NA_TILES)             /* unsigned keep count per tile */
-#define NA_BO    (NA_BK + ((4L*NA_TILES + 255)/256)*256) /* unsigned long long offset per tile */
-#define NA_ACC   (NA_BO + ((8L*NA_TILES + 255)/256)*256) /* sqb_acc_t */
-#define NA_MISC  (NA_ACC + 256)                      /* base, fallback count */
-#define NA_END   (NA_MISC + 256)
+#define NA_BP    (NA_STT + NA_UP(NA_CH))             /* sqb_part_t per tile */
+#define NA_BK    (NA_BP + NA_UP(sizeof(sqb_part_t)*NA_TILES))   /* unsigned keep count per tile */
+#define NA_BO    (NA_BK + NA_UP(4L*NA_TILES))        /* unsigned long long offset per tile */
+#define NA_ACC   (NA_BO + NA_UP(8L*NA_TILES))        /* sqb_acc_t */
+#define NA_MISC  (NA_ACC + NA_UP(sizeof(sqb_acc_t))) /* base, fallback count */
+#define NA_END   (NA_MISC + 256L)
+static_assert(NA_END <= SQB_NOALLOC_BYTES, "the scratch layout must fit the array the header states");
+static_assert(2*255*sizeof(double) <= 4096, "the lattice tables (|k| <= 127) must fit their slot");
+static_assert(sizeof(sqb_acc_t) <= 256 && 2*sizeof(unsigned long long) <= 256, "accumulator slots");
 
-static __device__ __align__(256) unsigned char sqb_noalloc_scratch[NA_END];
+static __device__ __align__(256) unsigned char sqb_noalloc_scratch[SQB_NOALLOC_BYTES];
 
 extern "C" int sqb_level_tail(const void *cells, long nchildren, int D, int st, int last, int abskip, double pw, double thr,
                               const double *v, const double *uu, const unsigned char *stt,
                               void *bp, unsigned *bkeep, unsigned long long *boff, sqb_acc_t *acc, unsigned long long *base,
                               void *next, long next_cap, void *stream);
 extern "C" size_t sqb_level_tile_bytes(void);
+extern "C" long sqb_level_tile_children(void);
 extern "C" void sqb_set_error_msg(const char *msg);
 
 #define NA_MAXDEV 64
@@ -69,7 +78,12 @@ extern "C" int sqb_level_noalloc(const char *graph, double h, int K, const void 
         sqb_set_error_msg(msg); return SQB_NOALLOC_BAD_ARG;
     }
     const long nch = ncell << D;
-    if(nch > NA_CH || sqb_level_tile_bytes() > 128){
+    /* the tail kernels' tile size is fixed at build time; the layout above holds NA_TILES of them */
+    if(sqb_level_tile_children() != SQB_TILE || sqb_level_tile_bytes() != sizeof(sqb_part_t)){
+        sqb_set_error_msg("sqb_level_noalloc: the library's level-tail tiles differ from this file's layout (a build mismatch)");
+        return SQB_NOALLOC_SETUP;
+    }
+    if(nch > NA_CH){
         snprintf(msg, sizeof msg, "sqb_level_noalloc: %ld cells of D=%d give %ld children, more than the fixed scratch holds "
                  "(%ld children per call): split the cells into several calls", ncell, D, nch, (long)NA_CH);
         sqb_set_error_msg(msg); return SQB_NOALLOC_TOO_BIG;

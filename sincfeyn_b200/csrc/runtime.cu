@@ -40,6 +40,7 @@ static thread_local char g_err[512];
     return (int)e_; } } while(0)
 
 extern "C" const char *sqb_last_error(void){ return g_err; }
+extern "C" void sqb_set_error_msg(const char *msg);        /* the text sqb_error() returns (engine.cpp) */
 
 extern "C" const sqb_graph_t *sqb_find_graph(const char *name){
     for(int i = 0; i < SQB_NALL; i++) if(!strcmp(SQB_ALL[i]->name, name) || !strcmp(SQB_ALL[i]->volkov, name)) return SQB_ALL[i];
@@ -754,6 +755,29 @@ extern "C" void sqb_gg_launch(const sqb_graph_t *g, void *st, long n, const shor
     a.X = EX; a.Wt = NULL; a.K = K; a.H = H; a.raw = 1; a.skip = skip; a.v = of; a.ab = oab;
     size_t smem = 2*(2*K + 1)*sizeof(double);
     g->f64(&a, grid_for(g, 0, n, smem), 128, smem, st);
+}
+
+/* GG_<graph>'s launcher with the FP64 build chosen (0 as written, 2 contracted) */
+extern "C" int sqb_plugin_launch(const char *graph, int form, cudaStream_t st, long n, const short *k, const unsigned char *skip,
+                                 const double *EX, int K, double H, double *of, double *oab, int cmode, int cst){
+    const sqb_graph_t *g = sqb_find_graph(graph);
+    if(!g || (form != 0 && form != 2) || (form == 2 && !g->f64_fma) || K < 0 || K > 127){
+        snprintf(g_err, sizeof g_err, "sqb_plugin_launch: no graph %s with FP64 build %d (or K %d outside 0..127)", graph, form, K);
+        sqb_set_error_msg(g_err);
+        return -1;
+    }
+    if(n <= 0) return 0;
+    if(sqb_dev_init(0)){ sqb_set_error_msg(g_err); return -1; }
+    sqb_eval_t a; memset(&a, 0, sizeof a);
+    a.pts = k; a.n = cmode ? (n >> g->D) : n; a.esize = 2; a.stride = g->D; a.flag_at = -1; a.cells = cmode; a.st = cst;
+    a.X = EX; a.Wt = NULL; a.K = K; a.H = H; a.raw = 1; a.skip = skip; a.v = of; a.ab = oab;
+    const size_t smem = 2*(2*K + 1)*sizeof(double);
+    launch_f64(g, form, &a, grid_for(g, form, n, smem), smem, st);
+    const cudaError_t e = cudaGetLastError();
+    if(e != cudaSuccess){
+        snprintf(g_err, sizeof g_err, "sqb_plugin_launch: %s", cudaGetErrorString(e)); sqb_set_error_msg(g_err); return (int)e; }
+    G.launches++;
+    return 0;
 }
 
 /* pointwise evaluation (parity checks): n points given by their variables, FP64 (SQ_AB = ab) or

@@ -32,14 +32,20 @@ Fixtures
                                 (`run 2.0 13 1e-4 GRAPH`, SINCQED_SYM unset = auto; the search's nodes only
                                 need K >= 6), and folded sums (SINCQED_SYM unset, SINCQED_KEEPBT=1) with
                                 top = 2 so that kept orbits go on to a second refinement level
+  all3_h0.7_N139_eps1e-12.json  `sincqed run 0.7 139 1e-12 GRAPH` for the 41 three-loop integrals (the headline
+                                workload), -ffp-contract=off build, SINCQED_SYM=0, SINCQED_KEEPBT=1, default
+                                top = 2: every results column, the fallback count and the host wall time
+                                (an hour or more on 8 cores; resumable, see all3())
 
-    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold scale predict]   # default: all of them
+    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold scale predict all3]
+    (default: all but all3)
 """
 import json
 import os
 import re
 import subprocess
 import sys
+import tempfile
 
 import numpy as np
 
@@ -187,8 +193,66 @@ def fold():
         json.dump(d, f, indent=1)
 
 
+ALL3 = (0.7, 139, 1e-12)
+ALL3_FILE = os.path.join(OUT, 'all3_h0.7_N139_eps1e-12.json')
+
+
+def all3():
+    """`sincqed run 0.7 139 1e-12 GRAPH` for each of the 41 integrals of all3 (default top = 2, K = 72): the
+    -ffp-contract=off build, SINCQED_SYM=0 (the unfolded point set) and SINCQED_KEEPBT=1 (one boundary
+    table: the exact grow), one graph per process with checkpoints every 15 min so that a stopped run
+    resumes.  The file is rewritten after every graph, and graphs already in it are not run again.  Each
+    row keeps the reference's wall time on this host (time_s) with the host's thread count and CPU."""
+    h, N, eps = ALL3
+    d = {'command': 'run 0.7 139 1e-12 GRAPH', 'h': h, 'N': N, 'eps': eps, 'top': 2,
+         'env': {'SINCQED_SYM': '0', 'SINCQED_KEEPBT': '1'}, 'binary': 'sincqed-exact (-ffp-contract=off)',
+         'threads': os.cpu_count(), 'cpu': _cpu_model(), 'rows': []}
+    if os.path.exists(ALL3_FILE):
+        with open(ALL3_FILE) as f:
+            d['rows'] = json.load(f)['rows']
+    done = {r['name'] for r in d['rows']}
+    ck = os.path.join(tempfile.gettempdir(), 'sincfeyn_golden_ckpt')
+    os.makedirs(ck, exist_ok=True)
+    for g in _set_members('all3'):
+        if g in done:
+            continue
+        env = dict(d['env'], SINCQED_CKPT='900', SINCQED_CKPT_DIR=ck)
+        rows, out = refpy.run(refpy.SINCQED_EXACT, h, N, eps, [g], env=env, timeout=6*3600)
+        r = with_log(rows, out)[0]
+        d['rows'].append(r)
+        with open(ALL3_FILE, 'w') as f:
+            json.dump(d, f, indent=1)
+        print('%s %+.16e evals %d %.1f s' % (g, r['value'], r['evals'], r['time_s']), flush=True)
+    d['set_sum'] = sum(r['value']*r['w'] for r in d['rows'])
+    d['reference_time_s'] = sum(r['time_s'] for r in d['rows'])
+    with open(ALL3_FILE, 'w') as f:
+        json.dump(d, f, indent=1)
+
+
+def _set_members(sel):
+    """the integrals of a loop-order group in the reference's registry order: its `list` output filtered
+    by the selector rule of driver/graphs.c:19-21 (allL: L = L, all3 without the w3_ checks)"""
+    assert sel in ('all2', 'all3')
+    env = dict(os.environ, SINCQED_LOG='-', SINCQED_RESULTS='-')
+    out = subprocess.run([refpy.SINCQED_EXACT, 'list'], env=env, stdout=subprocess.PIPE, text=True,
+                         check=True).stdout
+    L = 'L=' + sel[-1]
+    return [t[0] for t in (l.split() for l in out.splitlines() if l.startswith('  '))
+            if len(t) > 1 and t[1] == L and not t[0].startswith('w3_')]
+
+
+def _cpu_model():
+    try:
+        with open('/proc/cpuinfo') as f:
+            return next(l.split(':', 1)[1].strip() for l in f if l.startswith('model name'))
+    except (OSError, StopIteration):
+        return None
+
+
 if __name__ == '__main__':
     parts = sys.argv[1:] or ['all2', 'boxsum', 'pointwise', 'synth', 'fold', 'scale', 'predict']
+    if 'all3' in parts:
+        all3()
     if 'all2' in parts:
         all2()
     if 'boxsum' in parts:

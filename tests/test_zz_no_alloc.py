@@ -71,12 +71,21 @@ def existing_level(L, cells_dev, n, next_dev, cap, last, thr):
     return np.array(sums), [acc.ne, acc.keep, acc.nq, acc.unres, acc.skipped, acc.overflow]
 
 
-def noalloc_level(L, cells_dev, n, next_dev, cap, last, thr):
-    sums = (C.c_double * 12)()
-    counts = (C.c_longlong * 6)()
+def noalloc_lib():
+    """the library with the entry point's argument and result types declared (each test sets them, so that
+    any test runs alone)"""
+    L = sq.lib()
+    L.sqb_error.restype = C.c_char_p
+    L.sqb_level_noalloc.restype = C.c_int
     L.sqb_level_noalloc.argtypes = [C.c_char_p, C.c_double, C.c_int, C.c_void_p, C.c_long, C.c_int, C.c_int,
                                     C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                     C.c_int, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p]
+    return L
+
+
+def noalloc_level(L, cells_dev, n, next_dev, cap, last, thr):
+    sums = (C.c_double * 12)()
+    counts = (C.c_longlong * 6)()
     rc = L.sqb_level_noalloc(GRAPH.encode(), H, K, cells_dev, n, ST, last, float(ST**5), thr, ABSERR, NEARF,
                              DDSLACK, 1, 0, 1, next_dev, cap, sums, counts, None)
     assert rc == 0, L.sqb_error()
@@ -86,8 +95,7 @@ def noalloc_level(L, cells_dev, n, next_dev, cap, last, thr):
 @pytest.mark.parametrize('last', [0, 1])
 def test_noalloc_matches_the_allocating_level_pass(last):
     import torch
-    L = sq.lib()
-    L.sqb_error.restype = C.c_char_p
+    L = noalloc_lib()
     pts = cells_box()
     n = pts.shape[0]
     cells = torch.from_numpy(pts.copy()).cuda()
@@ -114,8 +122,7 @@ def test_noalloc_matches_the_allocating_level_pass(last):
 
 def test_noalloc_rejects_a_batch_beyond_its_scratch():
     import torch
-    L = sq.lib()
-    L.sqb_error.restype = C.c_char_p
+    L = noalloc_lib()
     n = (1 << 18)//32 + 1                                      # one cell more than the scratch holds
     cells = torch.zeros((n, 12), dtype=torch.int8, device='cuda')
     sums = (C.c_double * 12)()
