@@ -288,12 +288,19 @@ def run_single(args, sq, L):
         print(json.dumps({'workload': 'points', 'graph': g, 'prec': args.prec, 'points': args.npoints,
                           'sum_abs_f': float(np.nansum(np.abs(f if args.prec != 1 else f[:, 0])))}), flush=True)
         return
-    sq.hsum(g, H, N_PTS, EPS)
+    h = args.h or H
+    N = args.N or (2*math.ceil(48/h - 1e-9) + 1 if args.h else N_PTS)
+    kw = {'split': args.split}
+    sq.hsum(g, h, N, EPS, **kw)
     L.sqb_timer_start()
-    r = sq.hsum(g, H, N_PTS, EPS)
+    r = sq.hsum(g, h, N, EPS, **kw)
     ms = L.sqb_timer_stop()
-    print(json.dumps({'workload': 'single', 'graph': g, 'h': H, 'N': N_PTS, 'ms': ms, 'points': r['nev'],
-                      'f64_ms': r['f64_ms'], 'levels_ms': sum(r['lev_ms']), 'top_ms': 1e3*r['t_top']}), flush=True)
+    a1, a0 = sq.flops(g, 1), sq.flops(g, 0)
+    fl = (r['nev'] - r['abskipped'])*a1 + r['abskipped']*a0
+    print(json.dumps({'workload': 'single', 'graph': g, 'h': h, 'N': N, 'split': args.split, 'ms': ms,
+                      'points': r['nev'], 'value': r['S'][0], 'f64_ms': r['f64_ms'], 'f64_launches': r['f64_launches'],
+                      'f64_tflops': fl/(r['f64_ms']*1e-3)/1e12 if r['f64_ms'] else None,
+                      'levels_ms': sum(r['lev_ms']), 'top_ms': 1e3*r['t_top']}), flush=True)
 
 
 SYN_D = (5, 8, 11)
@@ -379,6 +386,10 @@ def main():
     ap.add_argument('--graph', default='g3_00', help='--workload single/points: the graph')
     ap.add_argument('--prec', type=int, default=2, help='--workload points: 0 FP64 as written, 2 contracted, 1 dd')
     ap.add_argument('--npoints', type=int, default=1 << 22, help='--workload points: number of nodes')
+    ap.add_argument('--split', type=int, default=0, help='--workload single: the FP64 pass form of a graph with '
+                    'node passes (0 one kernel, 1 passes, 2 lockstep)')
+    ap.add_argument('--h', type=float, default=0.0, help='--workload single: h (default 0.7)')
+    ap.add_argument('--N', type=int, default=0, help='--workload single: N (default 2ceil(48/h)+1)')
     ap.add_argument('--workload', default='all3', choices=['all3', 'mixed', 'synth', 'vp4', 'single', 'points'],
                     help='all3: the headline line; mixed: the mixed batch, one-at-a-time vs concurrent; '
                          'synth: the synthetic microbenchmark and its precision table; vp4: the four-loop '

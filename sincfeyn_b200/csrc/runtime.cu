@@ -198,7 +198,11 @@ static void fill_eval(sqb_eval_t *a, const sqb_test_t *t){
 
 /* whether a batch's FP64 pass runs in passes (the graph has them, they are asked for, a level batch) */
 static inline bool use_split(const sqb_graph_t *g, const sqb_eval_t *a, const sqb_test_t *t){
-    return t->split && g->nparts > 0 && a->cells && !t->alldd;
+    return t->split == 1 && g->nparts > 0 && a->cells && !t->alldd;
+}
+/* whether a level batch's FP64 pass runs the graph's lockstep kernel (split = 2, contracted form) */
+static inline bool use_lockstep(const sqb_graph_t *g, const sqb_eval_t *a, const sqb_test_t *t){
+    return t->split == 2 && t->fma && g->f64_ls && g->attr_ls && a->cells && !t->alldd;
 }
 
 /* FP64 pass (or the all-dd pass) and the fallback pass for one batch already described by a */
@@ -231,6 +235,12 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
             CKR(cudaGetLastError());
         }
         G.launches += g->nparts;
+    } else if(use_lockstep(g, a, t)){
+        sqb_kattr_t at; memset(&at, 0, sizeof at); int per = 2;
+        if(g->attr_ls(128, smem, &at) && at.blocks_per_sm > 0) per = at.blocks_per_sm;
+        const long want = (npts + 127)/128, full = (long)G.nsm*per;
+        g->f64_ls(a, (int)(want < full ? want : full), 128, smem, G.s);
+        CKR(cudaGetLastError());
     } else {
         const int w = f64_which(g, t->fma);
         launch_f64(g, w, a, grid_for(g, w, npts, smem), smem, G.s);
@@ -581,7 +591,8 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
          * pass: the reduce kernel sums every tile) */
         int can = 0;
         const long cap = grid_cap(g, f64_which(g, L->t.fma), 2*(2*G.K + 1)*sizeof(double), &can);
-        const bool fused = !L->t.alldd && can && !use_split(g, &a, &L->t) && nch >= 2*SQB_TILE*cap;
+        const bool fused = !L->t.alldd && can && !use_split(g, &a, &L->t) && !use_lockstep(g, &a, &L->t) &&
+                           nch >= 2*SQB_TILE*cap;
         /* the predictor at the last level: which children to leave out, and their tiers */
         if(pon){
             if(sqb_vtab_predict(L->vt, cells, nc, D, L->st, G.K, L->thr, L->predict, L->esok, L->sym, G.cfl,
