@@ -24,7 +24,7 @@ JSON line (rank 0):
              kernel's double path, counted by the code generator; skipped |.| sums counted as skipped) over
              their event-timed launches, against this device's FP64 FMA rate measured by a probe kernel
   cpu_baseline  the reference's own OpenMP CPU build (oracle/_ref/sincqed) on this host's cores, on a
-             bounded sample of the same workload (integrals of D = 5, 5, 6, 7), with its rate per D
+             bounded sample of the same workload (integrals of D = 5, 6, 6, 7), with its rate per D
   precision  the error of the results: a sample's FP64 + dd values against all-double-double GPU runs of
              the same integrals (two D = 7 graphs; --alldd-full: the whole set) with both forms' times, the
              set sum against the analytic A1^(6), and every integral against the reference CPU run of the
@@ -61,7 +61,7 @@ sys.path.insert(0, ROOT)
 
 H, N_PTS, EPS = 0.7, 139, 1e-12
 SET = 'all3'
-# the CPU sample: three-loop integrals of D = 5, 5, 6 and 7 at the workload's (h, N, eps); by points it is
+# the CPU sample: three-loop integrals of D = 5, 6, 6 and 7 at the workload's (h, N, eps); by points it is
 # mostly D = 7, as the set is (13 of its 41 integrals, about nine tenths of its points)
 CPU_SAMPLE = ['g3_07', 'v3_01', 'g3_01', 'g3_00']
 # the precision sample: FP64 + dd against all-dd, two D = 7 graphs among them
@@ -162,7 +162,7 @@ def run_reference(args, rank):
             'value': v, 'unit': 'points/s', 'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': 1e3*sec/args.steps, 'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None,
             'dtype': 'f64+dd', 'data': 'the reference kernels (kernels/g3, kernels/v3), no external data',
-            'config': {'workload': 'all3 at h=%g N=%d eps=%g: a sample, one integral per step cycling over %s (D = 5, 5, 6, 7)'
+            'config': {'workload': 'all3 at h=%g N=%d eps=%g: a sample, one integral per step cycling over %s (D = 5, 6, 6, 7)'
                                    % (H, N_PTS, EPS, ','.join(CPU_SAMPLE)),
                        'cpu': 'oracle/_ref/sincqed (reference CPU build, OpenMP)'},
             'cpu_baseline': {'value': v, 'unit': 'points/s', 'cores': threads, 'kind': 'reference',
@@ -189,37 +189,57 @@ def mixed_jobs(sq):
 
 
 def run_mixed(args, sq, L):
-    """--workload mixed: the batch one integral at a time (one worker) against the tuned concurrent
-    batch (sqb_hsum_batch); device time of each whole batch, points/s, and the two runs' values, which
-    must be identical (each integral's arithmetic does not depend on the schedule)."""
+    """--workload mixed: the batch one integral at a time (one worker), as a concurrent batch (the tuned
+    worker count, each integral alone) and grouped (each graph's four h as one group, sqb_hsum_group: its
+    refinement levels in shared launches over the four integrals, tiles from a device queue); device time
+    of each whole batch, points/s, and the runs' values, which must be identical (each integral's
+    arithmetic does not depend on the schedule).  The tuner runs a calibration sample (every 8th graph's
+    four integrals) once per candidate (workers, grouped or not) and picks the fastest."""
     import torch
     jobs = mixed_jobs(sq)
     for g in sorted({j[0] for j in jobs}):
         sq.preload(g)
-    sample = jobs[::8]
-    # warm-up: the calibration sample once per candidate is the tuner's own run
-    best, rates = sq.batch_tune(sample, (1, 2, 4, 6, 8))
+    graphs = sorted({j[0] for j in jobs})
+    sample = [j for j in jobs if j[0] in graphs[::8]]
+    # warm-up and tuning: the calibration sample once per candidate
+    rates = {}
+    best, best_rate = None, -1.0
+    for grp in (0, 1):
+        b, r = sq.batch_tune(sample, (1, 2, 4, 6, 8), group=grp)
+        for w, v in r.items():
+            rates['%s%d' % ('group_' if grp else '', w)] = v
+            if v > best_rate:
+                best, best_rate = (w, grp), v
     torch.cuda.synchronize()
     clocks = Clocks(0)
     seq, ms_seq = sq.hsum_batch(jobs, workers=1)
-    bat, ms_bat = sq.hsum_batch(jobs, workers=best)
+    bat, ms_bat = sq.hsum_batch(jobs, workers=best[0])
+    grp, ms_grp = sq.hsum_batch(jobs, workers=best[0], group=1)
+    tuned, ms_tuned = (grp, ms_grp) if best[1] else (bat, ms_bat)
     clk = clocks.stop()
     nev = sum(r['nev'] for r in seq)
-    same = all(all(x == y or (x != x and y != y) for x, y in zip(a['S'], b['S'])) and a['nev'] == b['nev']
-               for a, b in zip(seq, bat))
+
+    def ident(x, y):
+        return all(all(a == b or (a != a and b != b) for a, b in zip(p['S'], q['S'])) and p['nev'] == q['nev']
+                   for p, q in zip(x, y))
     info = {g['name']: g for g in sq.graphs()}
     per_h = {}
-    for j, r in zip(jobs, bat):
+    for j, r in zip(jobs, tuned):
         per_h.setdefault(j[1], [0.0, 0])
         per_h[j[1]][0] += r['S'][0]*info[j[0]]['weight']
         per_h[j[1]][1] += r['nev']
     line = {'workload': 'mixed', 'metric': 'integrand points/s of the mixed batch (all2+all3 x h=1.0,0.9,0.8,0.7)',
-            'value': nev/(ms_bat*1e-3), 'unit': 'points/s', 'n_gpus': 1, 'higher_is_better': True,
+            'value': nev/(ms_tuned*1e-3), 'unit': 'points/s', 'n_gpus': 1, 'higher_is_better': True,
             'integrals': len(jobs), 'points': nev,
-            'batched': {'workers': best, 'device_s': ms_bat*1e-3, 'points_s': nev/(ms_bat*1e-3)},
             'one_at_a_time': {'workers': 1, 'device_s': ms_seq*1e-3, 'points_s': nev/(ms_seq*1e-3)},
-            'speedup': ms_seq/ms_bat, 'identical_results': same,
-            'tuner': {'sample': '%d integrals (every 8th)' % len(sample), 'points_s_by_workers': rates, 'chosen': best},
+            'concurrent': {'workers': best[0], 'device_s': ms_bat*1e-3, 'points_s': nev/(ms_bat*1e-3),
+                           'speedup_vs_one_at_a_time': ms_seq/ms_bat},
+            'grouped': {'workers': best[0], 'device_s': ms_grp*1e-3, 'points_s': nev/(ms_grp*1e-3),
+                        'speedup_vs_one_at_a_time': ms_seq/ms_grp,
+                        'note': 'each graph\'s four h as one sqb_hsum_group: shared level launches, tiles from a device queue'},
+            'identical_results': ident(seq, bat) and ident(seq, grp),
+            'tuner': {'sample': '%d integrals (every 8th graph, its four h)' % len(sample), 'points_s': rates,
+                      'chosen': {'workers': best[0], 'grouped': bool(best[1])}},
             'sums_by_h': {str(h): {'sum': v[0], 'points': v[1]} for h, v in sorted(per_h.items())},
             'clocks': clk, 'dtype': 'f64+dd', 'data': 'the reference kernels (kernels/g2, g3, v3)',
             'config': {'workload': 'all2+all3 at h in %s, N=2ceil(48/h)+1, eps=%g, default top' % (list(MIX_H), EPS)}}

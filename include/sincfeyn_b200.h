@@ -95,7 +95,12 @@ typedef struct {
     double predict;        /* SINCQED_PREDICT = alpha (0 = off, the default): at the last level a child whose mean
                               |f| over the corners of its 2h cube (values of the level before, driver/sum.c:64-69)
                               is below alpha*thr is not evaluated; a controlled extra pruning loss */
+    int group;             /* sqb_hsum_batch: 1 = the integrals of one graph (up to SQB_GROUP_MAX, e.g. the graph at
+                              several h) run as one group (sqb_hsum_group), their refinement levels in shared
+                              launches that take tiles of every integral from a device queue; 0 (default) = each
+                              integral alone.  The results are the same bit for bit */
 } sqb_opts_t;
+#define SQB_GROUP_MAX 8
 #define SQB_CKPT_STOPPED 2 /* sqb_hsum's return code under ckpt_stop */
 
 /* res_t of the reference (driver/sq.h:111) and the per-graph log counters (driver/main.c:58-65) */
@@ -146,6 +151,14 @@ typedef struct {
 } sqb_job_t;
 int  sqb_hsum_batch(const sqb_job_t *jobs, int n, const sqb_opts_t *o, int workers, sqb_result_t *res, int *rcs,
                     double *device_ms);
+/* Several integrals of ONE graph (n <= SQB_GROUP_MAX; e.g. the graph at several h) as one group: their
+ * top levels one after another, then every refinement level as one sequence of launches over all the
+ * integrals that have it (the FP64 and double-double kernels take tiles of every integral from a device
+ * queue; one reduce, one finish with one block per integral, one scatter).  Each result (res[j], rcs[j]) is
+ * bit for bit the one sqb_hsum gives alone.  No counterpart in the reference.  A group with a checkpoint
+ * (ckpt_every > 0), the predictor, the all-dd form or the pass split runs its integrals one after another.
+ * Returns 0, or the number of failed jobs (sqb_error() names the first). */
+int  sqb_hsum_group(const sqb_job_t *jobs, int n, const sqb_opts_t *o, sqb_result_t *res, int *rcs);
 /* the batch tuner: runs the calibration jobs once per candidate worker count, rate[c] = evaluated points
  * per second of device time; *best = the fastest candidate.  Returns 0 or a batch error. */
 int  sqb_batch_tune(const sqb_job_t *jobs, int n, const sqb_opts_t *o, const int *cand, int ncand, double *rate,

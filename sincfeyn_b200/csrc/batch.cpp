@@ -17,6 +17,9 @@
  * integral at small h reach tens of GB) is not an error of the batch: it is run again after the queue
  * is drained, alone on the device, by the calling thread.
  *
+ * With opts.group the units of work are the integrals of one graph (up to SQB_GROUP_MAX, e.g. the graph at
+ * several h), each run by sqb_hsum_group: its refinement levels are shared launches over all of them.
+ *
  * The tuner runs a calibration list (normally a few integrals of the batch) once per candidate worker
  * count and returns the count with the highest evaluated points per second of device time. */
 #include <atomic>
@@ -39,6 +42,7 @@ namespace {
 
 struct Batch {
     const sqb_job_t *jobs = nullptr; int n = 0, nw = 0;
+    std::vector<std::vector<int>> units;     /* opts.group: the jobs of one graph, run by one sqb_hsum_group */
     sqb_opts_t o;
     sqb_result_t *res = nullptr; int *rcs = nullptr;
     std::vector<int> order;
@@ -73,16 +77,25 @@ void serve(Batch *b, int id){
     if(!ok) err = std::string("worker ") + std::to_string(id) + ": " + sqb_last_error();
     while(ok){
         const int k = b->next.fetch_add(1);
-        if(k >= b->n) break;
-        const int j = b->order[k];
-        const sqb_job_t &J = b->jobs[j];
-        b->rcs[j] = sqb_hsum(J.graph, J.h, J.N, J.eps, J.top, &b->o, &b->res[j]);
-        if(b->rcs[j]){
+        if(k >= (int)b->order.size()) break;
+        std::vector<int> js;
+        if(b->units.empty()) js.push_back(b->order[k]); else js = b->units[b->order[k]];
+        if(js.size() == 1){
+            const sqb_job_t &J = b->jobs[js[0]];
+            b->rcs[js[0]] = sqb_hsum(J.graph, J.h, J.N, J.eps, J.top, &b->o, &b->res[js[0]]);
+        } else {
+            std::vector<sqb_job_t> uj; std::vector<sqb_result_t> ur(js.size()); std::vector<int> uc(js.size());
+            for(int j : js) uj.push_back(b->jobs[j]);
+            sqb_hsum_group(uj.data(), (int)js.size(), &b->o, ur.data(), uc.data());
+            for(size_t q = 0; q < js.size(); q++){ b->res[js[q]] = ur[q]; b->rcs[js[q]] = uc[q]; }
+        }
+        for(int j : js){
+            if(!b->rcs[j]) continue;
             std::lock_guard<std::mutex> lk(b->m);
             if(out_of_memory(sqb_error())) b->retry.push_back(j);
             else {
                 b->failures++;
-                if(b->err.empty()) b->err = std::string(J.graph) + ": " + sqb_error();
+                if(b->err.empty()) b->err = std::string(b->jobs[j].graph) + ": " + sqb_error();
             }
         }
     }
@@ -126,10 +139,24 @@ extern "C" int sqb_hsum_batch(const sqb_job_t *jobs, int n, const sqb_opts_t *o_
         rcs[j] = 0; memset(&res[j], 0, sizeof res[j]);
     }
     Batch b;
-    b.jobs = jobs; b.n = n; b.nw = workers; b.o = o; b.res = res; b.rcs = rcs; b.left = workers;
-    b.order.resize(n);
-    for(int j = 0; j < n; j++) b.order[j] = j;
-    std::stable_sort(b.order.begin(), b.order.end(), [&](int x, int y){ return jobs[x].cost > jobs[y].cost; });
+    b.jobs = jobs; b.n = n; b.nw = workers; b.o = o; b.res = res; b.rcs = rcs;
+    std::vector<double> cost;
+    if(o.group){
+        /* the jobs of each graph in list order, SQB_GROUP_MAX at a time; a unit costs its jobs' sum */
+        std::vector<std::string> names;
+        for(int j = 0; j < n; j++){
+            size_t u = 0;
+            while(u < names.size() && (names[u] != jobs[j].graph || b.units[u].size() >= SQB_GROUP_MAX)) u++;
+            if(u == names.size()){ names.push_back(jobs[j].graph); b.units.push_back({}); cost.push_back(0); }
+            b.units[u].push_back(j); cost[u] += jobs[j].cost;
+        }
+    } else for(int j = 0; j < n; j++) cost.push_back(jobs[j].cost);
+    const int nu = (int)cost.size();
+    if(workers > nu) workers = nu;
+    b.nw = workers; b.left = workers;
+    b.order.resize(nu);
+    for(int u = 0; u < nu; u++) b.order[u] = u;
+    std::stable_sort(b.order.begin(), b.order.end(), [&](int x, int y){ return cost[x] > cost[y]; });
     b.ends.assign(workers, nullptr); b.ended.assign(workers, 0);
     cudaStream_t s = (cudaStream_t)sqb_dev_stream();
     int rc = 0;

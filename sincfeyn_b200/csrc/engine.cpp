@@ -227,131 +227,165 @@ static int sym_nodes(void *ctx, long n, const int *k, double *f, double *ab){
     return sqb_eval_points_impl(R.g, n, sf.data(), 0, 1, f, ab);
 }
 
-extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top, const sqb_opts_t *opts, sqb_result_t *res){
-    memset(res, 0, sizeof *res);
-    Run R; R.g = sqb_find_graph(graph);
-    if(!R.g) FAIL("no graph %s in this build", graph);
-    if(opts) R.o = *opts; else sqb_default_opts(&R.o);
-    if(sqb_dev_init(R.o.device)) FAIL("device: %s", sqb_last_error());
-    if(top < 0){ top = 1; while(top < 2 && (1 << (top + 1))*h <= 3.0*(1 + 1e-9)) top++; }   /* driver/main.c:211-215 */
-    R.D = R.g->D; R.h = h; R.eps = eps; R.top = top;
-    if(R.D >= SQB_MAXD) FAIL("D=%d needs MAXD > 12", R.D);
-    const int m = 1 << (top + 1); int K = (N - 1)/2; K = ((K + m - 1)/m)*m;   /* driver/lattice.c:16 */
-    if(K > 127) FAIL("N = %d gives K = %d; points are stored in 8 bits, so K <= 127 (N <= 255)", N, K);
-    R.K = K;
-    R.X.resize(2*K + 1); R.Wt.resize(2*K + 1);
-    for(int k = -K; k <= K; k++){
-        if(R.g->zlattice){ R.X[k + K] = k*h; R.Wt[k + K] = h; }
-        else { R.X[k + K] = exp(k*h); R.Wt[k + K] = R.X[k + K]*h; }
-    }
-    if(sqb_dev_tables(R.X.data(), R.Wt.data(), K)) FAIL("device: %s", sqb_last_error());
-    /* the symmetry fold's group (driver/sum.c:566-592), before the run's clock starts as there */
-    sqb_sym_t sym; memset(&sym, 0, sizeof sym); sym.n = 1;
-    res->sym_order = 1;
-    VtabGuard vtg;
-    if(R.o.predict > 0) R.vt = &vtg.t;
-    if(R.o.sym && *R.o.sym){
-        static thread_local int el[SQB_SYMG*SQB_MAXD];
-        const int n = sqb_sym_find(R.D, sym_nodes, &R, R.o.sym, el, res->sym_desc, sizeof res->sym_desc, &res->sym_worst,
-                                   res->sym_msg, sizeof res->sym_msg);
-        if(n < 0) FAIL("symmetry search: device: %s", sqb_last_error());
-        sym.n = n; res->sym_order = n;
-        for(int e = 0; e < n; e++) for(int i = 0; i < SQB_MAXD; i++) sym.g[e][i] = (signed char)el[e*SQB_MAXD + i];
-    }
-    double t0 = now();
-    const unsigned long long l0 = sqb_launch_count() + sqb_top_launches();
-    { double a, b; long c; sqb_kernel_times(&a, &b, &c, 1); }
-    /* a checkpoint of this run (same graph, h, eps, N, top, D, K) resumes it (driver/sum.c:596-606) */
-    char ckfn[4096] = ""; sqb_ckpt_t ck; memset(&ck, 0, sizeof ck); int resumed = 0;
-    if(R.o.ckpt_every > 0){
-        sqb_ckpt_name(ckfn, sizeof ckfn, R.o.ckpt_dir, R.g->name);
-        const int lr = sqb_ckpt_load(ckfn, &ck);
-        if(lr == 1 && !strcmp(ck.name, R.g->name) && ck.h == h && ck.eps == eps && ck.N == N && ck.top == top &&
-           ck.dim == R.D && ck.k == K && ck.lev >= 0 && ck.lev < top && ck.next >= 0 && ck.next <= ck.ncur && ck.nl >= 1) resumed = 1;
-        else {
-            if(lr == 1) sqb_ckpt_free(&ck);
-            if(lr && R.o.verbose) fprintf(stderr, "# checkpoint %s is for a different run or damaged: ignored\n", ckfn);
+/* One integral's run, in phases: begin() (lattice, symmetry group, checkpoint, box_zero, grow and dilate,
+ * or the resumed state), then per refinement level prep() (the level's sqb_level_t and next list) and
+ * done() (the level's sums, its checkpoint, the lists swapped), then end() (the result).  sqb_hsum runs
+ * them for one integral; sqb_hsum_group runs several integrals of one graph with their levels in shared
+ * launches.  Every early return releases the device lists and the checkpoint (destructor). */
+struct Integral {
+    Run R; sqb_result_t *res = NULL; sqb_sym_t sym; VtabGuard vtg;
+    int N = 0, top = 0, K = 0;
+    double t0 = 0, tl0 = 0; unsigned long long l0 = 0;
+    char ckfn[4096] = ""; sqb_ckpt_t ck; int resumed = 0;
+    sqb_pt_t *dcur = NULL, *dnext = NULL; long ncur = 0, next_cap = 0;
+    double Slev[16]; int nl = 0, esok = 0, lev0 = -1; long cnext = 0;
+    sqb_acc_t acc0;
+    double es1 = 0, es2 = 0, ah = 0, uu = 0;
+    long nkeep0 = 0;
+    double *dtab = NULL;                       /* this integral's tables on the device (group levels) */
+    Integral(){ memset(&sym, 0, sizeof sym); memset(&ck, 0, sizeof ck); memset(&acc0, 0, sizeof acc0); }
+    ~Integral(){ sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_dev_free(dtab); sqb_ckpt_free(&ck); }
+    Integral(const Integral &) = delete;
+    Integral &operator=(const Integral &) = delete;
+
+    /* 0: the levels follow; 1: finished at the top (zero integrand, or nothing to sum); -1: error */
+    int begin(const char *graph, double h, int N_, double eps, int top_, const sqb_opts_t *opts, sqb_result_t *res_, int tables){
+        res = res_; N = N_;
+        memset(res, 0, sizeof *res);
+        R.g = sqb_find_graph(graph);
+        if(!R.g) FAIL("no graph %s in this build", graph);
+        if(opts) R.o = *opts; else sqb_default_opts(&R.o);
+        if(sqb_dev_init(R.o.device)) FAIL("device: %s", sqb_last_error());
+        top = top_;
+        if(top < 0){ top = 1; while(top < 2 && (1 << (top + 1))*h <= 3.0*(1 + 1e-9)) top++; }   /* driver/main.c:211-215 */
+        R.D = R.g->D; R.h = h; R.eps = eps; R.top = top;
+        if(R.D >= SQB_MAXD) FAIL("D=%d needs MAXD > 12", R.D);
+        const int m = 1 << (top + 1); K = (N - 1)/2; K = ((K + m - 1)/m)*m;   /* driver/lattice.c:16 */
+        if(K > 127) FAIL("N = %d gives K = %d; points are stored in 8 bits, so K <= 127 (N <= 255)", N, K);
+        R.K = K;
+        R.X.resize(2*K + 1); R.Wt.resize(2*K + 1);
+        for(int k = -K; k <= K; k++){
+            if(R.g->zlattice){ R.X[k + K] = k*h; R.Wt[k + K] = h; }
+            else { R.X[k + K] = exp(k*h); R.Wt[k + K] = R.X[k + K]*h; }
         }
-    }
-    sqb_pt_t *dcur = NULL; long ncur = 0;
-    double Slev[16]; int nl = 0; int esok, lev0 = top - 1; long cnext = 0;
-    sqb_acc_t acc0; memset(&acc0, 0, sizeof acc0);
-    if(resumed){
-        for(int i = 0; i < 3; i++) res->S[i] = NAN;
-        res->nev = ck.nev; res->ref = ck.ref; res->prune = ck.prune; res->trunc = ck.trunc; res->kept_top = ck.kept_top;
-        R.nq = ck.nq; res->abskipped = ck.cnt[1]; res->pskip = ck.cnt[0];
-        if(R.vt && ck.vcap > 0 && ck.vs && sqb_vtab_upload(R.vt, ck.vs, ck.vcap, ck.vn, sqb_dev_stream())){
-            sqb_ckpt_free(&ck); FAIL("predictor: %s", sqb_vtab_error()); }
-        nl = ck.nl; for(int i = 0; i < nl; i++) Slev[i] = ck.Slev[i];
-        esok = ck.esok; lev0 = ck.lev; cnext = ck.next; t0 -= ck.t;
-        ncur = ck.ncur;
-        dcur = (sqb_pt_t*)sqb_dev_alloc((size_t)(ncur ? ncur : 1)*sizeof(sqb_pt_t));
-        if(!dcur || (ncur && sqb_dev_upload(dcur, ck.cur, (size_t)ncur*sizeof(sqb_pt_t)))){
-            sqb_dev_free(dcur); sqb_ckpt_free(&ck); FAIL("device copy of the checkpoint's %ld cells failed", ncur); }
-        if(cnext > 0){         /* a level in progress: its partial sums carry on */
-            acc0.S[0] = ck.s; acc0.A[0] = ck.a; acc0.drop[0] = ck.drop; acc0.u[0] = ck.u;
-            acc0.b1[0] = ck.es[0]; acc0.b2[0] = ck.es[1]; acc0.ne = ck.ne; acc0.nq = ck.q;
+        if(sqb_dev_tables(R.X.data(), R.Wt.data(), K)) FAIL("device: %s", sqb_last_error());
+        if(tables){
+            dtab = (double*)sqb_dev_alloc(2*(2*K + 1)*sizeof(double));
+            if(!dtab || sqb_dev_upload(dtab, R.X.data(), (2*K + 1)*sizeof(double)) ||
+               sqb_dev_upload(dtab + 2*K + 1, R.Wt.data(), (2*K + 1)*sizeof(double))) FAIL("device copy of the lattice tables failed");
         }
-        if(R.o.verbose) fprintf(stderr, "# resuming %s from checkpoint: refine to step %dh, cell %ld of %ld\n",
-                                R.g->name, 1 << ck.lev, ck.next, ck.ncur);
-        res->t_top = 0;
-    } else {
-        set_test(R, R.o.abserr0);
-        int zero = 0;
-        if(box_zero(R, top, &res->nev, &zero)) return -1;
-        if(zero){ res->zero = 1; res->t = now() - t0; return 0; }
-        GrowOut go;
-        if(grow(R, top, eps*1e-3, &go, &dcur, &ncur)) return -1;
-        if(vt_check(R, E_, sizeof E_)){ sqb_dev_free(dcur); return -1; }
-        res->nev += go.nev; res->ref = go.A; res->prune = go.drop;
-        if(top == 0 && go.gshn) res->prune = fabs(go.gshs);
-        if(go.A == 0){ sqb_dev_free(dcur); res->t = now() - t0; res->nq = R.nq; res->unresdrop = R.unresdrop; return 0; }
-        { double r = go.e2 > 0 ? go.e1/go.e2 : 0; res->trunc = (r > 0 && r < 1) ? go.e1*r/(1 - r) : go.e1; }
-        for(int i = 0; i < 3; i++) res->S[i] = NAN;
-        Slev[nl++] = go.S;
-        res->kept_top = ncur;
-        res->t_top = now() - t0;
-        esok = R.D < SQB_MAXD && top > 0;
+        /* the symmetry fold's group (driver/sum.c:566-592), before the run's clock starts as there */
+        sym.n = 1;
+        res->sym_order = 1;
+        if(R.o.predict > 0) R.vt = &vtg.t;
+        if(R.o.sym && *R.o.sym){
+            static thread_local int el[SQB_SYMG*SQB_MAXD];
+            const int n = sqb_sym_find(R.D, sym_nodes, &R, R.o.sym, el, res->sym_desc, sizeof res->sym_desc, &res->sym_worst,
+                                       res->sym_msg, sizeof res->sym_msg);
+            if(n < 0) FAIL("symmetry search: device: %s", sqb_last_error());
+            sym.n = n; res->sym_order = n;
+            for(int e = 0; e < n; e++) for(int i = 0; i < SQB_MAXD; i++) sym.g[e][i] = (signed char)el[e*SQB_MAXD + i];
+        }
+        t0 = now();
+        l0 = sqb_launch_count() + sqb_top_launches();
+        { double a, b; long c; sqb_kernel_times(&a, &b, &c, 1); }
+        /* a checkpoint of this run (same graph, h, eps, N, top, D, K) resumes it (driver/sum.c:596-606) */
+        if(R.o.ckpt_every > 0){
+            sqb_ckpt_name(ckfn, sizeof ckfn, R.o.ckpt_dir, R.g->name);
+            const int lr = sqb_ckpt_load(ckfn, &ck);
+            if(lr == 1 && !strcmp(ck.name, R.g->name) && ck.h == h && ck.eps == eps && ck.N == N && ck.top == top &&
+               ck.dim == R.D && ck.k == K && ck.lev >= 0 && ck.lev < top && ck.next >= 0 && ck.next <= ck.ncur && ck.nl >= 1) resumed = 1;
+            else {
+                if(lr == 1) sqb_ckpt_free(&ck);
+                memset(&ck, 0, sizeof ck);
+                if(lr && R.o.verbose) fprintf(stderr, "# checkpoint %s is for a different run or damaged: ignored\n", ckfn);
+            }
+        }
+        lev0 = top - 1;
+        if(resumed){
+            for(int i = 0; i < 3; i++) res->S[i] = NAN;
+            res->nev = ck.nev; res->ref = ck.ref; res->prune = ck.prune; res->trunc = ck.trunc; res->kept_top = ck.kept_top;
+            R.nq = ck.nq; res->abskipped = ck.cnt[1]; res->pskip = ck.cnt[0];
+            if(R.vt && ck.vcap > 0 && ck.vs && sqb_vtab_upload(R.vt, ck.vs, ck.vcap, ck.vn, sqb_dev_stream()))
+                FAIL("predictor: %s", sqb_vtab_error());
+            nl = ck.nl; for(int i = 0; i < nl; i++) Slev[i] = ck.Slev[i];
+            esok = ck.esok; lev0 = ck.lev; cnext = ck.next; t0 -= ck.t;
+            ncur = ck.ncur;
+            dcur = (sqb_pt_t*)sqb_dev_alloc((size_t)(ncur ? ncur : 1)*sizeof(sqb_pt_t));
+            if(!dcur || (ncur && sqb_dev_upload(dcur, ck.cur, (size_t)ncur*sizeof(sqb_pt_t))))
+                FAIL("device copy of the checkpoint's %ld cells failed", ncur);
+            if(cnext > 0){         /* a level in progress: its partial sums carry on */
+                acc0.S[0] = ck.s; acc0.A[0] = ck.a; acc0.drop[0] = ck.drop; acc0.u[0] = ck.u;
+                acc0.b1[0] = ck.es[0]; acc0.b2[0] = ck.es[1]; acc0.ne = ck.ne; acc0.nq = ck.q;
+            }
+            if(R.o.verbose) fprintf(stderr, "# resuming %s from checkpoint: refine to step %dh, cell %ld of %ld\n",
+                                    R.g->name, 1 << ck.lev, ck.next, ck.ncur);
+            res->t_top = 0;
+        } else {
+            set_test(R, R.o.abserr0);
+            int zero = 0;
+            if(box_zero(R, top, &res->nev, &zero)) return -1;
+            if(zero){ res->zero = 1; res->t = now() - t0; return 1; }
+            GrowOut go;
+            if(grow(R, top, eps*1e-3, &go, &dcur, &ncur)) return -1;
+            if(vt_check(R, E_, sizeof E_)) return -1;
+            res->nev += go.nev; res->ref = go.A; res->prune = go.drop;
+            if(top == 0 && go.gshn) res->prune = fabs(go.gshs);
+            if(go.A == 0){ res->t = now() - t0; res->nq = R.nq; res->unresdrop = R.unresdrop; return 1; }
+            { double r = go.e2 > 0 ? go.e1/go.e2 : 0; res->trunc = (r > 0 && r < 1) ? go.e1*r/(1 - r) : go.e1; }
+            for(int i = 0; i < 3; i++) res->S[i] = NAN;
+            Slev[nl++] = go.S;
+            res->kept_top = ncur;
+            res->t_top = now() - t0;
+            esok = R.D < SQB_MAXD && top > 0;
+        }
+        /* the levels on the device */
+        set_test(R, fmax(R.o.abserr0, R.o.abrel*eps*res->ref));    /* driver/sum.c:651 */
+        tl0 = now();
+        return 0;
     }
-    /* the levels on the device */
-    set_test(R, fmax(R.o.abserr0, R.o.abrel*eps*res->ref));    /* driver/sum.c:651 */
-    sqb_pt_t *dnext = NULL; long next_cap = 0;
-    const double tl0 = now(); double es1 = 0, es2 = 0, ah = 0, uu = 0;
-    for(int lev = lev0; lev >= 0; lev--){
+
+    /* the level lev (lev0 >= lev >= 0): its sqb_level_t, the next level's list allocated */
+    int prep(int lev, sqb_level_t *L, sqb_acc_t *acc){
         const int st = 1 << lev, last = lev == 0;
         /* resumed in mid-level: cells [cnext, ncur) remain, and the checkpoint's kept cells come first */
-        const long nkeep0 = lev == lev0 ? ck.nnxt : 0, c0 = lev == lev0 ? cnext : 0;
-        sqb_level_t L; memset(&L, 0, sizeof L);
-        L.g = R.g; L.cells = dcur + c0; L.ncell = ncur - c0; L.st = st; L.last = last;
-        L.pw = pow(st, R.D); L.thr = eps*res->ref*1e-2; L.t = R.t; L.max_children = R.o.max_children;
-        L.sym = &sym;
+        nkeep0 = lev == lev0 ? ck.nnxt : 0;
+        const long c0 = lev == lev0 ? cnext : 0;
+        memset(L, 0, sizeof *L);
+        L->g = R.g; L->cells = dcur + c0; L->ncell = ncur - c0; L->st = st; L->last = last;
+        L->pw = pow(st, R.D); L->thr = R.eps*res->ref*1e-2; L->t = R.t; L->max_children = R.o.max_children;
+        L->sym = &sym;
+        L->X = dtab; L->Wt = dtab ? dtab + 2*K + 1 : NULL; L->K = K;
         /* the predictor: the level before the last stores its values, the last level uses them
          * (driver/sum.c:385, 739) */
         if(R.vt){
-            L.vt = R.vt; L.vput = lev == 1; L.esok = esok;
-            if(last) L.predict = R.o.predict;
-            if(L.vput && sqb_vtab_reserve(R.vt, (ncur - c0) << R.D, sqb_dev_stream())){
-                sqb_dev_free(dcur); sqb_ckpt_free(&ck); FAIL("predictor: %s", sqb_vtab_error()); }
+            L->vt = R.vt; L->vput = lev == 1; L->esok = esok;
+            if(last) L->predict = R.o.predict;
+            if(L->vput && sqb_vtab_reserve(R.vt, (ncur - c0) << R.D, sqb_dev_stream())) FAIL("predictor: %s", sqb_vtab_error());
         }
         if(!last){
             double want = (double)(ncur - c0)*(double)(1L << R.D) + nkeep0;
             double room = 0.35*MEMSHARE*(double)sqb_dev_total_bytes()/sizeof(sqb_pt_t);
             next_cap = (long)(want < room ? want : room) + 1;
             dnext = (sqb_pt_t*)sqb_dev_alloc(next_cap*sizeof(sqb_pt_t));
-            if(!dnext){ sqb_dev_free(dcur); sqb_ckpt_free(&ck); FAIL("device allocation of the next level (%ld cells) failed", next_cap); }
-            if(nkeep0 && (nkeep0 >= next_cap || sqb_dev_upload(dnext, ck.nxt, (size_t)nkeep0*sizeof(sqb_pt_t)))){
-                sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); FAIL("device copy of the checkpoint's kept cells failed"); }
-            L.next = dnext + nkeep0; L.next_cap = next_cap - nkeep0;
+            if(!dnext) FAIL("device allocation of the next level (%ld cells) failed", next_cap);
+            if(nkeep0 && (nkeep0 >= next_cap || sqb_dev_upload(dnext, ck.nxt, (size_t)nkeep0*sizeof(sqb_pt_t))))
+                FAIL("device copy of the checkpoint's kept cells failed");
+            L->next = dnext + nkeep0; L->next_cap = next_cap - nkeep0;
         }
-        sqb_acc_t acc; if(lev == lev0) acc = acc0; else memset(&acc, 0, sizeof acc);
-        long nn = 0; double ms = 0;
-        if(sqb_dev_level(&L, &acc, &nn, &ms)){ sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); FAIL("device: %s", sqb_last_error()); }
-        if(acc.overflow){ sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); FAIL("level %d: %ld kept cells exceed the device list (%ld)", lev, nn, next_cap); }
+        if(lev == lev0) *acc = acc0; else memset(acc, 0, sizeof *acc);
+        return 0;
+    }
+
+    /* after the level's sums acc (nn kept children, ms device milliseconds): 0, -1, or SQB_CKPT_STOPPED */
+    int done(int lev, const sqb_acc_t &acc, long nn, double ms){
+        const int st = 1 << lev, last = lev == 0;
+        if(acc.overflow) FAIL("level %d: %ld kept cells exceed the device list (%ld)", lev, nn, next_cap);
         nn += nkeep0;
         Slev[nl++] = ddv(acc.S);
         res->prune += ddv(acc.drop); res->nev += (long)acc.ne; R.nq += (long)acc.nq; R.unresdrop += (long)acc.unres;
         res->abskipped += (long)acc.skipped; res->pskip += (long)acc.pskip;
-        if(vt_check(R, E_, sizeof E_)){ sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); return -1; }
+        if(vt_check(R, E_, sizeof E_)) return -1;
         if(res->nlev < 16){ res->lev_evals[res->nlev] = (long)acc.ne; res->lev_ms[res->nlev] = ms; res->nlev++; }
         if(last){ ah = ddv(acc.A); uu = ddv(acc.u); es1 = ddv(acc.b1); es2 = ddv(acc.b2); }
         if(R.o.verbose) fprintf(stderr, "# %s level step %dh: %ld cells, %llu evals, %llu fallback, %ld kept, %.1f ms\n",
@@ -359,11 +393,10 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
         if(R.o.ckpt_every > 0 && !last){
             /* the state between this level and the next, as the reference saves it (driver/sum.c:797-799) */
             std::vector<sqb_pt_t> host((size_t)nn);
-            if(nn && sqb_dev_download(host.data(), dnext, (size_t)nn*sizeof(sqb_pt_t))){
-                sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); FAIL("device: %s", sqb_last_error()); }
+            if(nn && sqb_dev_download(host.data(), dnext, (size_t)nn*sizeof(sqb_pt_t))) FAIL("device: %s", sqb_last_error());
             sqb_ckpt_t c; memset(&c, 0, sizeof c);
             snprintf(c.name, sizeof c.name, "%s", R.g->name);
-            c.h = h; c.eps = eps; c.N = N; c.top = top; c.dim = R.D; c.k = K;
+            c.h = R.h; c.eps = R.eps; c.N = N; c.top = top; c.dim = R.D; c.k = K;
             c.lev = lev - 1; c.next = 0;
             c.s = Slev[nl - 1]; c.a = ddv(acc.A); c.drop = ddv(acc.drop); c.u = ddv(acc.u);
             c.ne = (long)acc.ne; c.q = (long)acc.nq;
@@ -380,32 +413,100 @@ extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top,
             if(R.vt && R.vt->tab){
                 long vn = 0, full = 0;
                 vs.resize((size_t)R.vt->cap*SQB_CKPT_VSLOT);
-                if(sqb_vtab_counts(R.vt, &vn, &full, sqb_dev_stream()) || sqb_vtab_download(R.vt, vs.data(), sqb_dev_stream())){
-                    sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck); FAIL("predictor: %s", sqb_vtab_error()); }
+                if(sqb_vtab_counts(R.vt, &vn, &full, sqb_dev_stream()) || sqb_vtab_download(R.vt, vs.data(), sqb_dev_stream()))
+                    FAIL("predictor: %s", sqb_vtab_error());
                 c.vs = vs.data(); c.vcap = R.vt->cap; c.vn = vn;
             }
             if(sqb_ckpt_save(ckfn, &c) && R.o.verbose) fprintf(stderr, "# warning: could not write checkpoint %s\n", ckfn);
             if(R.o.ckpt_stop){
-                sqb_dev_free(dcur); sqb_dev_free(dnext); sqb_ckpt_free(&ck);
                 snprintf(E_, sizeof E_, "stopped after the checkpoint %s (ckpt_stop)", ckfn);
                 return SQB_CKPT_STOPPED;
             }
         }
         sqb_dev_free(dcur); dcur = dnext; dnext = NULL; ncur = last ? 0 : nn;
+        return 0;
     }
-    sqb_dev_free(dcur);
-    sqb_ckpt_free(&ck);
-    if(R.o.ckpt_every > 0) remove(ckfn);          /* the graph is finished (driver/sum.c:804) */
-    res->t_levels = now() - tl0;
-    if(top > 0){ res->unres = sqrt(uu); res->Ah = ah; }
-    else res->unres = R.u;            /* top = 0: the grow's sum of squares as it stands (driver/sum.c:795) */
-    res->S[0] = Slev[nl - 1]; res->S[1] = nl > 1 ? Slev[nl - 2] : NAN; res->S[2] = nl > 2 ? Slev[nl - 3] : NAN;
-    res->es1 = es1; res->es2 = es2; res->esok = esok;
-    res->nq = R.nq; res->unresdrop = R.unresdrop;
-    sqb_kernel_times(&res->f64_ms, &res->dd_ms, &res->f64_launches, 1);
-    res->launches = (long)(sqb_launch_count() + sqb_top_launches() - l0);
-    res->t = now() - t0;
+
+    void end(){
+        sqb_dev_free(dcur); dcur = NULL;
+        if(R.o.ckpt_every > 0) remove(ckfn);          /* the graph is finished (driver/sum.c:804) */
+        res->t_levels = now() - tl0;
+        if(top > 0){ res->unres = sqrt(uu); res->Ah = ah; }
+        else res->unres = R.u;            /* top = 0: the grow's sum of squares as it stands (driver/sum.c:795) */
+        res->S[0] = Slev[nl - 1]; res->S[1] = nl > 1 ? Slev[nl - 2] : NAN; res->S[2] = nl > 2 ? Slev[nl - 3] : NAN;
+        res->es1 = es1; res->es2 = es2; res->esok = esok;
+        res->nq = R.nq; res->unresdrop = R.unresdrop;
+        sqb_kernel_times(&res->f64_ms, &res->dd_ms, &res->f64_launches, 1);
+        res->launches = (long)(sqb_launch_count() + sqb_top_launches() - l0);
+        res->t = now() - t0;
+    }
+};
+
+extern "C" int sqb_hsum(const char *graph, double h, int N, double eps, int top, const sqb_opts_t *opts, sqb_result_t *res){
+    Integral I;
+    const int b = I.begin(graph, h, N, eps, top, opts, res, 0);
+    if(b) return b < 0 ? -1 : 0;
+    for(int lev = I.lev0; lev >= 0; lev--){
+        sqb_level_t L; sqb_acc_t acc;
+        if(I.prep(lev, &L, &acc)) return -1;
+        long nn = 0; double ms = 0;
+        if(sqb_dev_level(&L, &acc, &nn, &ms)) FAIL("device: %s", sqb_last_error());
+        const int rc = I.done(lev, acc, nn, ms);
+        if(rc) return rc;
+    }
+    I.end();
     return 0;
+}
+
+/* Several integrals of one graph (e.g. one graph at several h), their refinement levels in shared launches:
+ * the integrals' top levels run one after another on this thread's stream, then for lev from the highest
+ * down to 0 one sqb_dev_level_multi over the integrals that have that level.  Each result is bit for bit
+ * the one sqb_hsum gives alone; the level times (lev_ms) are those of the shared launches.  A group with a
+ * checkpoint or the predictor runs its integrals one after another. */
+extern "C" int sqb_hsum_group(const sqb_job_t *jobs, int n, const sqb_opts_t *opts, sqb_result_t *res, int *rcs){
+    sqb_opts_t o; if(opts) o = *opts; else sqb_default_opts(&o);
+    if(n <= 0) return 0;
+    int fails = 0;
+    bool seq = n == 1 || n > SQB_MAXINST || o.ckpt_every > 0 || o.predict > 0 || o.alldd || o.split == 1;
+    for(int j = 1; j < n && !seq; j++) seq = strcmp(jobs[j].graph, jobs[0].graph) != 0;
+    if(seq){
+        for(int j = 0; j < n; j++){ rcs[j] = sqb_hsum(jobs[j].graph, jobs[j].h, jobs[j].N, jobs[j].eps, jobs[j].top, &o, &res[j]); fails += rcs[j] != 0; }
+        return fails;
+    }
+    std::vector<Integral> I(n);
+    std::vector<int> live(n, 0);
+    int maxlev = -1;
+    for(int j = 0; j < n; j++){
+        rcs[j] = 0;
+        const int b = I[j].begin(jobs[j].graph, jobs[j].h, jobs[j].N, jobs[j].eps, jobs[j].top, &o, &res[j], 1);
+        if(b < 0){ rcs[j] = -1; fails++; continue; }
+        if(b == 0){ live[j] = 1; if(I[j].lev0 > maxlev) maxlev = I[j].lev0; }
+    }
+    char err[512] = "";
+    for(int lev = maxlev; lev >= 0; lev--){
+        sqb_level_t L[SQB_MAXINST]; sqb_acc_t acc[SQB_MAXINST]; long nn[SQB_MAXINST]; int who[SQB_MAXINST], m = 0;
+        for(int j = 0; j < n; j++){
+            if(!live[j] || lev > I[j].lev0) continue;
+            if(I[j].prep(lev, &L[m], &acc[m])){ rcs[j] = -1; fails++; live[j] = 0; if(!*err) snprintf(err, sizeof err, "%s: %s", jobs[j].graph, E_); continue; }
+            who[m++] = j;
+        }
+        if(!m) continue;
+        double ms = 0;
+        if(sqb_dev_level_multi(L, m, acc, nn, &ms)){
+            snprintf(E_, sizeof E_, "device: %s", sqb_last_error());
+            for(int q = 0; q < m; q++){ rcs[who[q]] = -1; live[who[q]] = 0; fails++; }
+            if(!*err) snprintf(err, sizeof err, "%s", E_);
+            continue;
+        }
+        for(int q = 0; q < m; q++){
+            const int j = who[q];
+            const int rc = I[j].done(lev, acc[q], nn[q], ms);
+            if(rc){ rcs[j] = rc; live[j] = 0; fails++; if(!*err) snprintf(err, sizeof err, "%s: %s", jobs[j].graph, E_); }
+        }
+    }
+    for(int j = 0; j < n; j++) if(live[j]) I[j].end();
+    if(fails && *err) snprintf(E_, sizeof E_, "%s", err);
+    return fails;
 }
 
 /* pointwise kernel evaluation for parity checks */

@@ -58,6 +58,15 @@ extern "C" const sqb_graph_t *sqb_graph_at(int i){ return i >= 0 && i < SQB_NALL
 typedef sqb_part_t part_t;
 static_assert(RTILE == SQB_TILE, "the reduce kernel's tiles are the FP64 kernel's");
 
+/* one integral of a multi-instance level batch, for the tail kernels: its children are the launch's
+ * [child0, child0 + n); its kept children go to next (cap cells), its sums to acc, its first kept slot to
+ * *base */
+typedef struct {
+    const signed char *cells; long n, child0;
+    int st, last; double pw, thr;
+    sqb_pt_t *next; long cap;
+    sqb_acc_t *acc; unsigned long long *base;
+} lvi_t;
 typedef struct {
     const signed char *cells;     /* device pt_t list (12 bytes per cell) */
     long n;                       /* children in this batch */
@@ -67,6 +76,9 @@ typedef struct {
     const unsigned char *stt;
     sqb_sym_t sym;                /* the symmetry fold (sym.n <= 1: off) */
     const unsigned char *cfl;     /* the predictor's per-child tiers at the last level (NULL: the parent's) */
+    int ninst;                    /* > 0: a multi-instance batch, the integrals in inst (the fields above that
+                                     describe one batch unused); 0: one batch */
+    lvi_t inst[SQB_MAXINST];
 } lvl_t;
 
 struct Dev {
@@ -84,6 +96,7 @@ struct Dev {
     long nbcap; part_t *bp; unsigned *bkeep; unsigned long long *boff; unsigned char *tfb;
     long ttcap; double *tt, *ta;   /* split FP64 pass: running sums per point */
     sqb_acc_t *acc; unsigned long long *base;
+    sqb_acc_t *accm; unsigned long long *basem, *queue;   /* multi-instance levels: per integral, tile queue */
     long dcap; sqb_pt_t *dpts; unsigned char *dskip;
     long hcap; sqb_pt_t *hpts; unsigned char *hskip, *hst; double *hv, *huu;
 };
@@ -134,6 +147,9 @@ extern "C" int sqb_dev_init(int device){
     CKR(cudaMalloc(&G.acc, sizeof(sqb_acc_t)));
     CKR(cudaMalloc(&G.base, sizeof(unsigned long long)));
     CKR(cudaMalloc(&G.nfb, sizeof(unsigned long long)));
+    CKR(cudaMalloc(&G.accm, SQB_MAXINST*sizeof(sqb_acc_t)));
+    CKR(cudaMalloc(&G.basem, SQB_MAXINST*sizeof(unsigned long long)));
+    CKR(cudaMalloc(&G.queue, sizeof(unsigned long long)));
     G.on = 1;
     return 0;
 }
@@ -206,8 +222,16 @@ static inline bool use_lockstep(const sqb_graph_t *g, const sqb_eval_t *a, const
 }
 
 /* FP64 pass (or the all-dd pass) and the fallback pass for one batch already described by a */
+/* dynamic shared memory of a launch: the tables of its integral(s), 2(2K+1) doubles each */
+static size_t table_bytes(const sqb_eval_t *a){
+    if(a->ninst <= 0) return 2*(2*(size_t)a->K + 1)*sizeof(double);
+    size_t w = 0;
+    for(int q = 0; q < a->ninst; q++) w += 2*(2*(size_t)a->inst[q].K + 1);
+    return w*sizeof(double);
+}
+
 static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, long npts){
-    size_t smem = 2*(2*G.K + 1)*sizeof(double);
+    size_t smem = table_bytes(a);
     sqb_dd_t d; memset(&d, 0, sizeof d);
     d.e = *a; d.dropunres = t->dropunres; d.uu = G.uu;
     if(t->alldd){
@@ -238,12 +262,17 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
     } else if(use_lockstep(g, a, t)){
         sqb_kattr_t at; memset(&at, 0, sizeof at); int per = 2;
         if(g->attr_ls(128, smem, &at) && at.blocks_per_sm > 0) per = at.blocks_per_sm;
-        const long want = (npts + 127)/128, full = (long)G.nsm*per;
+        const long want = a->ninst > 0 ? a->ntile : (npts + 127)/128, full = (long)G.nsm*per;
+        if(a->ninst > 0) CKR(cudaMemsetAsync(a->queue, 0, sizeof(unsigned long long), G.s));
         g->f64_ls(a, (int)(want < full ? want : full), 128, smem, G.s);
         CKR(cudaGetLastError());
     } else {
         const int w = f64_which(g, t->fma);
-        launch_f64(g, w, a, grid_for(g, w, npts, smem), smem, G.s);
+        if(a->ninst > 0){
+            CKR(cudaMemsetAsync(a->queue, 0, sizeof(unsigned long long), G.s));
+            const long cap = grid_cap(g, w, smem);
+            launch_f64(g, w, a, (int)(a->ntile < cap ? a->ntile : cap), smem, G.s);
+        } else launch_f64(g, w, a, grid_for(g, w, npts, smem), smem, G.s);
         CKR(cudaGetLastError());
     }
     if(ev) CKR(cudaEventRecord(ev[1], G.s));
@@ -365,24 +394,36 @@ extern "C" void sqb_kernel_times(double *f64_ms, double *dd_ms, long *f64_launch
 __device__ __forceinline__ sqdd shfl_dd(const sqdd &a, int off){
     return sqdd(__shfl_down_sync(0xffffffffu, a.hi, off), __shfl_down_sync(0xffffffffu, a.lo, off));
 }
-/* child i's coordinates k_d - st bit_d(b) (driver/sum.c:407) */
-__device__ __forceinline__ void child_of(const lvl_t &a, long i, int *k){
-    const long c = i >> a.D; const int b = (int)(i & ((1L << a.D) - 1));
-    const signed char *p = a.cells + c*SQB_MAXD;
-    for(int d = 0; d < a.D; d++) k[d] = p[d] - (((b >> d) & 1) ? a.st : 0);
+/* the integral of tile b of a batch (one batch: the batch itself, with child0 = 0) */
+__device__ __forceinline__ lvi_t lvl_inst(const lvl_t &a, long b){
+    lvi_t v;
+    if(a.ninst <= 0){
+        v.cells = a.cells; v.n = a.n; v.child0 = 0; v.st = a.st; v.last = a.last; v.pw = a.pw; v.thr = a.thr;
+        v.next = NULL; v.cap = 0; v.acc = NULL; v.base = NULL;
+        return v;
+    }
+    int k = 0;
+    for(int q = 1; q < a.ninst; q++) if(a.inst[q].child0 <= b*(long)RTILE) k = q;
+    return a.inst[k];
+}
+/* child il's coordinates k_d - st bit_d(b) (driver/sum.c:407) */
+__device__ __forceinline__ void child_of(const lvl_t &a, const lvi_t &L, long il, int *k){
+    const long c = il >> a.D; const int b = (int)(il & ((1L << a.D) - 1));
+    const signed char *p = L.cells + c*SQB_MAXD;
+    for(int d = 0; d < a.D; d++) k[d] = p[d] - (((b >> d) & 1) ? L.st : 0);
 }
 /* a present child's multiplicity: its orbit size under a fold, else 1 */
-__device__ __forceinline__ int child_weight(const lvl_t &a, long i){
+__device__ __forceinline__ int child_weight(const lvl_t &a, const lvi_t &L, long il){
     if(a.sym.n <= 1) return 1;
     int k[SQB_MAXD];
-    child_of(a, i, k);
+    child_of(a, L, il, k);
     return sqb_orbit_n(a.sym, k, a.D);
 }
 
-__device__ __forceinline__ int parent_tier(const lvl_t &a, long i){
+__device__ __forceinline__ int parent_tier(const lvl_t &a, const lvi_t &L, long i, long il){
     if(a.cfl) return (a.cfl[i] >> 1) & 3;
-    const long c = i >> a.D;
-    return (a.cells[c*SQB_MAXD + SQB_PFLAG] >> 1) & 3;
+    const long c = il >> a.D;
+    return (L.cells[c*SQB_MAXD + SQB_PFLAG] >> 1) & 3;
 }
 
 /* per tile of RTILE children: S = sum v*pw and the shadow-tier sums in double-double per thread (they
@@ -390,30 +431,32 @@ __device__ __forceinline__ int parent_tier(const lvl_t &a, long i){
  * then double-double across threads in a fixed tree.  Thread t of the tile takes children t, t + RT,
  * t + 2 RT, ... (each warp reads 256 contiguous bytes of v per step); the order is fixed, so a run is
  * reproducible. */
-__global__ void __launch_bounds__(RT) sqb_k_reduce(const lvl_t a, part_t *bp, unsigned *bkeep, const unsigned char *tfb){
+__global__ void __launch_bounds__(RT) sqb_k_reduce(const __grid_constant__ lvl_t a, part_t *bp, unsigned *bkeep,
+                                                   const unsigned char *tfb){
     if(tfb && !tfb[blockIdx.x]) return;      /* summed by the FP64 pass already (no fallback point in it) */
+    const lvi_t L = lvl_inst(a, blockIdx.x);
     const long t0 = blockIdx.x*(long)RTILE + threadIdx.x;
     sqdd S, b1, b2;
     double A = 0, dr = 0, uu = 0;
     unsigned ne = 0, nq = 0, nu = 0, nsk = 0, keep = 0;
     for(int j = 0; j < RPT; j++){
-        const long i = t0 + (long)j*RT;
-        if(i >= a.n) break;
+        const long i = t0 + (long)j*RT, il = i - L.child0;
+        if(il >= L.n) break;
         const unsigned char s = a.stt[i];
         if(!(s & SQB_PRESENT)) continue;
         /* a folded point stands for its orbit: (mw v) pw and mw |v| (driver/sum.c:734-745) */
-        const int mw = child_weight(a, i);
-        const double m = (double)mw, v = a.v[i], vp = (m*v)*a.pw, av = fabs(v);
+        const int mw = child_weight(a, L, il);
+        const double m = (double)mw, v = a.v[i], vp = (m*v)*L.pw, av = fabs(v);
         S = sqdd_add_d(S, vp); A += m*av; ne++;
         nsk += (s & SQB_SKIPPED) ? 1 : 0;
         if(s & SQB_FALLBACK){ nq++; uu += a.uu[i]; }
         if(s & SQB_UNRES) nu++;
-        if(a.last){
-            const int te = parent_tier(a, i);
+        if(L.last){
+            const int te = parent_tier(a, L, i, il);
             if(te >= 1) b1 = sqdd_add_d(b1, vp);
             if(te >= 2) b2 = sqdd_add_d(b2, vp);
-        } else if(av >= a.thr) keep += mw;
-        else dr += (m*av)*a.pw;
+        } else if(av >= L.thr) keep += mw;
+        else dr += (m*av)*L.pw;
     }
     sqdd Ad(A), dd(dr), ud(uu);
     for(int off = 16; off; off >>= 1){
@@ -451,11 +494,19 @@ __global__ void __launch_bounds__(RT) sqb_k_reduce(const lvl_t a, part_t *bp, un
     }
 }
 
-/* one CTA: the tiles' offsets (exclusive scan of their kept counts) and the batch's sums, in a fixed
- * order (each thread a contiguous run of tiles, then a fixed tree), added into the level accumulator;
- * *base = this batch's first slot in the next list */
-__global__ void __launch_bounds__(FT) sqb_k_finish(const part_t *bp, const unsigned *bkeep, long nb,
-                                                   unsigned long long *boff, sqb_acc_t *acc, unsigned long long *base){
+/* one CTA per integral: the tiles' offsets (exclusive scan of their kept counts) and the batch's sums, in
+ * a fixed order (each thread a contiguous run of tiles, then a fixed tree), added into the level
+ * accumulator; *base = this batch's first slot in the next list.  One batch (a.ninst = 0): its nb tiles
+ * into acc and base; a multi-instance batch: CTA k takes integral k's tiles into its own acc and base */
+__global__ void __launch_bounds__(FT) sqb_k_finish(const __grid_constant__ lvl_t a, const part_t *bp, const unsigned *bkeep,
+                                                   long nb, unsigned long long *boff, sqb_acc_t *acc,
+                                                   unsigned long long *base){
+    long tb = 0;
+    if(a.ninst > 0){
+        const lvi_t &L = a.inst[blockIdx.x];
+        tb = L.child0/RTILE; nb = (L.n + RTILE - 1)/RTILE; acc = L.acc; base = L.base;
+    }
+    bp += tb; bkeep += tb; boff += tb;
     const int t = threadIdx.x, w = t >> 5, l = t & 31;
     const long ch = (nb + FT - 1)/FT, j0 = t*ch, j1 = j0 + ch < nb ? j0 + ch : nb;
     sqdd x[6]; unsigned long long c[5] = {0, 0, 0, 0, 0};
@@ -500,15 +551,17 @@ __global__ void __launch_bounds__(FT) sqb_k_finish(const part_t *bp, const unsig
     }
 }
 
-__global__ void __launch_bounds__(RT) sqb_k_scatter(const lvl_t a, const unsigned long long *boff,
+__global__ void __launch_bounds__(RT) sqb_k_scatter(const __grid_constant__ lvl_t a, const unsigned long long *boff,
                                                     const unsigned long long *base, sqb_pt_t *next, long cap,
                                                     unsigned long long *overflow){
+    const lvi_t L = lvl_inst(a, blockIdx.x);
+    if(a.ninst > 0){ base = L.base; next = L.next; cap = L.cap; overflow = &L.acc->overflow; }
     const long t0 = blockIdx.x*(long)RTILE + threadIdx.x*(long)RPT;
     unsigned mask = 0; int cnt = 0;
     for(int j = 0; j < RPT; j++){
-        const long i = t0 + j;
-        if(i >= a.n) break;
-        if((a.stt[i] & SQB_PRESENT) && fabs(a.v[i]) >= a.thr){ mask |= 1u << j; cnt += child_weight(a, i); }
+        const long i = t0 + j, il = i - L.child0;
+        if(il >= L.n) break;
+        if((a.stt[i] & SQB_PRESENT) && fabs(a.v[i]) >= L.thr){ mask |= 1u << j; cnt += child_weight(a, L, il); }
     }
     /* block exclusive scan of cnt */
     __shared__ int ws[RT/32];
@@ -520,19 +573,19 @@ __global__ void __launch_bounds__(RT) sqb_k_scatter(const lvl_t a, const unsigne
     if(threadIdx.x == 0){ int s = 0; for(int j = 0; j < RT/32; j++){ int y = ws[j]; ws[j] = s; s += y; } }
     __syncthreads();
     unsigned long long o = *base + boff[blockIdx.x] + (unsigned long long)(ws[w] + x - cnt);
-    const double thr10 = 10*a.thr, thr100 = 100*a.thr;
+    const double thr10 = 10*L.thr, thr100 = 100*L.thr;
     for(int j = 0; j < RPT; j++){
         if(!(mask >> j & 1)) continue;
-        const long i = t0 + j;
-        const long c = i >> a.D;
-        const signed char *p = a.cells + c*SQB_MAXD;
+        const long i = t0 + j, il = i - L.child0;
+        const long c = il >> a.D;
+        const signed char *p = L.cells + c*SQB_MAXD;
         const unsigned char s = a.stt[i];
         const double av = fabs(a.v[i]);
         const int te = (p[SQB_PFLAG] >> 1) & 3, tv = (av >= thr10) + (av >= thr100);
         const int psk = (s & SQB_SKIPPED) ? 1 : 0, nr = (s & SQB_NEAR) ? 1 : 0;
         const signed char fl = (signed char)((a.abskip && (psk || !nr)) | ((te < tv ? te : tv) << 1));
         int k[SQB_MAXD];
-        child_of(a, i, k);
+        child_of(a, L, il, k);
         /* the child, then (under a fold) the other members of its orbit in group order, each once
          * (symorbit(), driver/sum.c:38-46), all with the child's flags (driver/sum.c:741-744) */
         const int ng = a.sym.n > 1 ? a.sym.n : 1;
@@ -615,7 +668,7 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
         const long nb = (nch + RTILE - 1)/RTILE;
         sqb_k_reduce<<<(unsigned)nb, RT, 0, G.s>>>(r, G.bp, G.bkeep, fused ? G.tfb : NULL);
         CKR(cudaGetLastError());
-        sqb_k_finish<<<1, FT, 0, G.s>>>(G.bp, G.bkeep, nb, G.boff, G.acc, G.base);
+        sqb_k_finish<<<1, FT, 0, G.s>>>(r, G.bp, G.bkeep, nb, G.boff, G.acc, G.base);
         CKR(cudaGetLastError());
         G.launches += 2;
         if(!L->last){
@@ -635,6 +688,130 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
     acc->ne += h.ne; acc->nq += h.nq; acc->unres += h.unres; acc->skipped += h.skipped; acc->keep += h.keep; acc->overflow += h.overflow;
     acc->pskip += h.pskip;
     *next_n = (long)h.keep;
+    return 0;
+}
+
+/* A level of several integrals of one graph at once (see sqb_rt.h).  Each integral keeps the batches,
+ * tiles and fused/unfused choice that sqb_dev_level would give it alone; round r launches batch r of every
+ * integral that has one, its children numbered integral after integral from tile boundaries. */
+extern "C" int sqb_dev_level_multi(const sqb_level_t *Ls, int n, sqb_acc_t *accs, long *next_n, double *ms){
+    if(n <= 0) return 0;
+    bool one_by_one = n == 1 || n > SQB_MAXINST;
+    const sqb_graph_t *g = Ls[0].g; const int D = g->D;
+    for(int k = 0; k < n && !one_by_one; k++){
+        const sqb_level_t &L = Ls[k];
+        one_by_one = L.g != g || L.t.alldd || L.t.split == 1 || L.predict > 0 || L.vput || L.st != Ls[0].st ||
+                     L.last != Ls[0].last || !L.X || !L.Wt || L.K < 1 || L.K > 127 || L.t.fma != Ls[0].t.fma ||
+                     L.t.split != Ls[0].t.split || L.t.abskip != Ls[0].t.abskip || L.t.abcheck != Ls[0].t.abcheck ||
+                     L.t.dropunres != Ls[0].t.dropunres || L.t.ddslack != Ls[0].t.ddslack ||
+                     ((L.sym && L.sym->n > 1) != (Ls[0].sym && Ls[0].sym->n > 1)) ||
+                     (L.sym && Ls[0].sym && L.sym->n > 1 && memcmp(L.sym, Ls[0].sym, sizeof(sqb_sym_t)));
+    }
+    if(one_by_one){
+        /* each integral on its own tables: the thread's current ones are lent the integral's device copy */
+        double tot = 0; int rc = 0;
+        double *sx = G.X, *sw = G.Wt; const int sk = G.K;
+        for(int k = 0; k < n && !rc; k++){
+            if(Ls[k].X){ G.X = (double*)Ls[k].X; G.Wt = (double*)Ls[k].Wt; G.K = Ls[k].K; }
+            double m = 0;
+            rc = sqb_dev_level(&Ls[k], &accs[k], &next_n[k], &m);
+            tot += m;
+            G.X = sx; G.Wt = sw; G.K = sk;
+        }
+        if(ms) *ms = tot;
+        return rc;
+    }
+    const sqb_level_t &L0 = Ls[0];
+    if(L0.sym && L0.sym->n > 1){
+        bool ok = L0.sym->n <= SQB_SYMG;
+        for(int e = 0; ok && e < L0.sym->n; e++) for(int i = 0; i < D; i++) ok = ok && L0.sym->g[e][i] >= 0 && L0.sym->g[e][i] < D;
+        if(!ok){ snprintf(g_err, sizeof g_err, "symmetry group: %d elements or an axis outside 0..%d", L0.sym->n, D - 1); return -1; }
+    }
+    /* per integral: cells per batch and the number of batches, as sqb_dev_level chooses them */
+    long ncb[SQB_MAXINST], nbat[SQB_MAXINST], capk[SQB_MAXINST]; int cank[SQB_MAXINST]; long rounds = 0;
+    const int which = f64_which(g, L0.t.fma);
+    for(int k = 0; k < n; k++){
+        const sqb_level_t &L = Ls[k];
+        long maxch = L.max_children > 0 ? L.max_children : (1L << 25);
+        if(maxch < (1L << D)) maxch = 1L << D;
+        long c = maxch >> D;
+        const size_t sm1 = 2*(2*(size_t)L.K + 1)*sizeof(double);
+        int can0 = 0;
+        const long cap0 = grid_cap(g, which, sm1, &can0);
+        const long round = (cap0*SQB_TILE) >> D;
+        if(can0 && round > 0 && c >= 2*round) c = (c/round)*round;
+        ncb[k] = c; capk[k] = cap0; cank[k] = can0;
+        nbat[k] = (L.ncell + c - 1)/c;
+        if(nbat[k] > rounds) rounds = nbat[k];
+    }
+    /* the largest round's children, each integral's batch from a tile boundary */
+    long maxtot = 0;
+    for(long r = 0; r < rounds; r++){
+        long tot = 0;
+        for(int k = 0; k < n; k++) if(r < nbat[k]){
+            const long nc = Ls[k].ncell - r*ncb[k] < ncb[k] ? Ls[k].ncell - r*ncb[k] : ncb[k];
+            tot += ((nc << D) + SQB_TILE - 1)/SQB_TILE*SQB_TILE;
+        }
+        if(tot > maxtot) maxtot = tot;
+    }
+    if(reserve_points(maxtot)) return -1;
+    CKR(cudaMemsetAsync(G.accm, 0, n*sizeof(sqb_acc_t), G.s));
+    CKR(cudaEventRecord(G.e0, G.s));
+    for(long r = 0; r < rounds; r++){
+        sqb_eval_t a; memset(&a, 0, sizeof a); fill_eval(&a, &L0.t);
+        a.esize = 1; a.stride = SQB_MAXD; a.flag_at = SQB_PFLAG; a.cells = 1;
+        if(L0.sym && L0.sym->n > 1) a.sym = *L0.sym;
+        a.part = G.bp; a.tkeep = G.bkeep; a.tfb = G.tfb; a.queue = G.queue;
+        lvl_t rl; memset(&rl, 0, sizeof rl);
+        rl.D = D; rl.abskip = L0.t.abskip; rl.v = G.v; rl.uu = G.uu; rl.stt = G.stt; rl.sym = a.sym;
+        long child0 = 0; int m = 0, toff = 0, last = 0, kof[SQB_MAXINST];
+        for(int k = 0; k < n; k++){
+            if(r >= nbat[k]) continue;
+            const sqb_level_t &L = Ls[k];
+            const long c0 = r*ncb[k], nc = L.ncell - c0 < ncb[k] ? L.ncell - c0 : ncb[k], nch = nc << D;
+            sqb_inst_t &I = a.inst[m];
+            I.pts = L.cells + c0; I.n = nc; I.child0 = child0; I.st = L.st; I.K = L.K; I.toff = toff;
+            I.fused = cank[k] && !use_lockstep(g, &a, &L.t) && nch >= 2*SQB_TILE*capk[k];
+            I.last = L.last; I.pw = L.pw; I.thr = L.thr; I.abserr = L.t.abserr; I.near_thr = L.t.nearf*L.t.abserr;
+            I.X = L.X; I.Wt = L.Wt;
+            lvi_t &V = rl.inst[m];
+            V.cells = (const signed char*)(L.cells + c0); V.n = nch; V.child0 = child0; V.st = L.st; V.last = L.last;
+            V.pw = L.pw; V.thr = L.thr; V.next = L.next; V.cap = L.next_cap; V.acc = G.accm + k; V.base = G.basem + k;
+            last = L.last; kof[m] = k;
+            toff += 2*(2*L.K + 1);
+            child0 += (nch + SQB_TILE - 1)/SQB_TILE*SQB_TILE;
+            m++;
+        }
+        (void)kof;
+        a.ninst = m; a.ntile = child0/SQB_TILE; rl.ninst = m;
+        /* the per-point thresholds of the first integral stand in the launch's own fields (unused by the
+         * kernels in a multi-instance launch) */
+        if(eval_batch(g, &a, &Ls[0].t, child0)) return -1;
+        sqb_k_reduce<<<(unsigned)a.ntile, RT, 0, G.s>>>(rl, G.bp, G.bkeep, G.tfb);
+        CKR(cudaGetLastError());
+        sqb_k_finish<<<(unsigned)m, FT, 0, G.s>>>(rl, G.bp, G.bkeep, 0, G.boff, NULL, NULL);
+        CKR(cudaGetLastError());
+        G.launches += 2;
+        if(!last){
+            sqb_k_scatter<<<(unsigned)a.ntile, RT, 0, G.s>>>(rl, G.boff, NULL, NULL, 0, NULL);
+            CKR(cudaGetLastError());
+            G.launches++;
+        }
+    }
+    CKR(cudaEventRecord(G.e1, G.s));
+    sqb_acc_t h[SQB_MAXINST];
+    CKR(cudaMemcpyAsync(h, G.accm, n*sizeof(sqb_acc_t), cudaMemcpyDeviceToHost, G.s));
+    CKR(cudaStreamSynchronize(G.s));
+    D2H += n*sizeof(sqb_acc_t);
+    float t = 0; cudaEventElapsedTime(&t, G.e0, G.e1); if(ms) *ms = t;
+    for(int k = 0; k < n; k++){
+        sqb_acc_t *acc = &accs[k];
+        double *src[6] = {h[k].S, h[k].A, h[k].drop, h[k].b1, h[k].b2, h[k].u}, *dst[6] = {acc->S, acc->A, acc->drop, acc->b1, acc->b2, acc->u};
+        for(int q = 0; q < 6; q++){ sqdd x = sqdd(dst[q][0], dst[q][1]) + sqdd(src[q][0], src[q][1]); dst[q][0] = x.hi; dst[q][1] = x.lo; }
+        acc->ne += h[k].ne; acc->nq += h[k].nq; acc->unres += h[k].unres; acc->skipped += h[k].skipped;
+        acc->keep += h[k].keep; acc->overflow += h[k].overflow; acc->pskip += h[k].pskip;
+        next_n[k] = (long)h[k].keep;
+    }
     return 0;
 }
 
@@ -908,7 +1085,7 @@ extern "C" int sqb_level_tail(const void *cells, long nchildren, int D, int st, 
     cudaStream_t s = (cudaStream_t)stream;
     sqb_k_reduce<<<(unsigned)nb, RT, 0, s>>>(r, (part_t*)bp, bkeep, NULL);
     CKR(cudaGetLastError());
-    sqb_k_finish<<<1, FT, 0, s>>>((const part_t*)bp, bkeep, nb, boff, acc, base);
+    sqb_k_finish<<<1, FT, 0, s>>>(r, (const part_t*)bp, bkeep, nb, boff, acc, base);
     CKR(cudaGetLastError());
     if(!last){
         sqb_k_scatter<<<(unsigned)nb, RT, 0, s>>>(r, boff, base, (sqb_pt_t*)next, next_cap, &acc->overflow);

@@ -37,6 +37,22 @@ typedef struct {
     unsigned long long ne, nq, unres, skipped;
 } sqb_part_t;
 
+/* One integral of a multi-instance level launch: the instances of one graph at several h (or several
+ * integrals of it) share a launch, the launch's children numbered instance after instance, each instance's
+ * range starting at a multiple of SQB_TILE so that no tile straddles two instances. */
+#define SQB_MAXINST 8
+typedef struct {
+    const void *pts;              /* its cells (device), pt_t layout */
+    long n;                       /* its cells in this launch */
+    long child0;                  /* its first child in the launch's numbering (a multiple of SQB_TILE) */
+    int st, K, toff, fused;       /* step; lattice half-width; offset of its tables in the launch's shared
+                                     table area (X then Wt, 2K+1 each); the FP64 kernel sums its tiles */
+    int last;
+    double pw, thr;               /* its level's weight step^D and keep threshold */
+    double abserr, near_thr;      /* its per-point test thresholds (ABSERR depends on the integral's Ref) */
+    const double *X, *Wt;         /* its tables (device, 2K+1 each) */
+} sqb_inst_t;
+
 typedef struct {
     const void *pts;
     long n;                       /* nodes, or cells */
@@ -68,6 +84,13 @@ typedef struct {
     sqb_sym_t sym;                /* cells only: the symmetry fold (sym.n <= 1: off) */
     const unsigned char *cfl;     /* cells only, the predictor at the last level (NULL: off): per child, bit 0 =
                                      not evaluated, bits 1-2 = its shadow tier */
+    /* multi-instance level launch (ninst >= 1, cells, level mode): the instances' own fields above are
+     * unused; the CTAs take tiles of SQB_TILE children from the device counter queue in turn, children
+     * numbered as sqb_inst_t says (ntile tiles in all).  ninst = 0: one batch described by the fields above */
+    int ninst;
+    long ntile;
+    unsigned long long *queue;
+    sqb_inst_t inst[SQB_MAXINST];
 } sqb_eval_t;
 
 /* The double-double kernel over a list of points of the same launch geometry (fb/nfb from the FP64

@@ -79,8 +79,18 @@ typedef struct {
      * the last level = leave out the children whose predicted mean is below predict*thr (esok: and cap
      * their tiers) */
     sqb_vtab_t *vt; int vput; double predict; int esok;
+    /* the integral's lattice tables on the device (2K+1 each), for sqb_dev_level_multi; sqb_dev_level uses
+     * the thread's current tables (sqb_dev_tables) */
+    const double *X, *Wt; int K;
 } sqb_level_t;
 int  sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n, double *ms);
+/* the same level of n <= SQB_MAXINST integrals of one graph at once (each L[i] as for sqb_dev_level, with
+ * its own tables, cells, lists and test thresholds): each launch of the FP64, double-double, reduce, finish
+ * and scatter kernels covers batch b of every integral that has one, the FP64 and double-double kernels
+ * taking tiles from a device queue.  Batches, tiles and summation order per integral are those of
+ * sqb_dev_level, so every result is bit for bit the one sqb_dev_level gives.  Integrals with the predictor
+ * or the pass split run one after another through sqb_dev_level. */
+int  sqb_dev_level_multi(const sqb_level_t *L, int n, sqb_acc_t *acc, long *next_n, double *ms);
 
 /* the same for n nodes already on the device (pts, skip device pointers); the values and status come
  * back to the host (v, stt) and stay on the device until the next evaluation (*v_dev, *stt_dev) */

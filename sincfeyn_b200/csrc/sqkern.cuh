@@ -54,62 +54,98 @@
 #endif
 #define SQB_QEPS 4.93e-32   /* double-double epsilon of the fallback's error model (driver/common.h:8) */
 
-/* coordinates and weight of point i; returns 0 for a child below the box, a child the predictor leaves
- * out or, under a symmetry fold, a child that is not the minimum of its orbit (driver/sum.c:405-416), else
- * the point's multiplicity (the orbit size; 1 without a fold) */
+/* The per-integral fields of a launch (sqb_inst_t) sit in shared memory: every thread of a CTA works on
+ * one integral at a time.  A launch over one batch (ninst = 0) has one record, made from its own fields;
+ * a multi-instance launch (ninst >= 1) has one per integral, with their tables side by side. */
+__device__ __forceinline__ void sqb_inst_of(const sqb_eval_t &a, sqb_inst_t *I){
+    I->pts = a.pts; I->n = a.n; I->child0 = 0; I->st = a.st; I->K = a.K; I->toff = 0; I->fused = 1;
+    I->last = a.last; I->pw = a.pw; I->thr = a.thr; I->abserr = a.abserr; I->near_thr = a.near_thr;
+    I->X = a.X; I->Wt = a.Wt;
+}
+/* the instance of global child index i (ninst >= 1): the last one whose range starts at or before i */
+__device__ __forceinline__ int sqb_inst_at(const sqb_eval_t &a, long i){
+    int k = 0;
+    for(int q = 1; q < a.ninst; q++) if(a.inst[q].child0 <= i) k = q;
+    return k;
+}
+/* shared-memory words of the tables of a launch: 2(2K+1) per integral */
+__host__ __device__ __forceinline__ int sqb_table_words(const sqb_eval_t &a){
+    if(a.ninst <= 0) return 2*(2*a.K + 1);
+    int w = 0;
+    for(int q = 0; q < a.ninst; q++) w += 2*(2*a.inst[q].K + 1);
+    return w;
+}
+
+/* coordinates and weight of point il of integral I (ig: its index in the launch, the same for one batch);
+ * returns 0 for a child below the box, a child the predictor leaves out or, under a symmetry fold, a child
+ * that is not the minimum of its orbit (driver/sum.c:405-416), else the point's multiplicity (the orbit
+ * size; 1 without a fold) */
 template<int D>
-__device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const double *sX, const double *sW,
-                                         long i, long *cell, double *sf, double *w){
+__device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const sqb_inst_t &I, const double *sX, const double *sW,
+                                         long il, long ig, long *cell, double *sf, double *w){
     long c; int b;
-    if(a.cells){ c = i >> D; b = (int)(i & ((1L << D) - 1)); } else { c = i; b = 0; }
+    if(a.cells){ c = il >> D; b = (int)(il & ((1L << D) - 1)); } else { c = il; b = 0; }
     *cell = c;
     if(a.sfin){
 #pragma unroll
-        for(int d = 0; d < D; d++) sf[d] = a.sfin[i*D + d];
+        for(int d = 0; d < D; d++) sf[d] = a.sfin[ig*D + d];
         *w = 1.0;
         return 1;
     }
     double ww = 1.0; bool in = true;
     int kk[D];
+    const int K = I.K, st = I.st;
     if(a.esize == 1){
-        const signed char *p = (const signed char*)a.pts + c*(long)a.stride;
+        const signed char *p = (const signed char*)I.pts + c*(long)a.stride;
 #pragma unroll
         for(int d = 0; d < D; d++){
-            int kd = p[d] - (((b >> d) & 1) ? a.st : 0);
+            int kd = p[d] - (((b >> d) & 1) ? st : 0);
             kk[d] = kd;
-            if(kd < -a.K){ in = false; kd = -a.K; }
-            sf[d] = sX[kd + a.K]; ww = ww*sW[kd + a.K];
+            if(kd < -K){ in = false; kd = -K; }
+            sf[d] = sX[kd + K]; ww = ww*sW[kd + K];
         }
     } else {
-        const short *p = (const short*)a.pts + c*(long)a.stride;
+        const short *p = (const short*)I.pts + c*(long)a.stride;
 #pragma unroll
         for(int d = 0; d < D; d++){
-            int kd = p[d] - (((b >> d) & 1) ? a.st : 0);
+            int kd = p[d] - (((b >> d) & 1) ? st : 0);
             kk[d] = kd;
-            if(kd < -a.K){ in = false; kd = -a.K; }
-            sf[d] = sX[kd + a.K]; ww = ww*sW[kd + a.K];
+            if(kd < -K){ in = false; kd = -K; }
+            sf[d] = sX[kd + K]; ww = ww*sW[kd + K];
         }
     }
     *w = ww;
     if(!in) return 0;
-    if(a.cfl && (a.cfl[i] & 1)) return 0;          /* left out by the predictor */
+    if(a.cfl && (a.cfl[ig] & 1)) return 0;          /* left out by the predictor */
     return a.cells && a.sym.n > 1 ? sqb_orbit<D>(a.sym, kk) : 1;
 }
 
 template<int D>
-__device__ __forceinline__ int sqb_skip(const sqb_eval_t &a, long c){
+__device__ __forceinline__ int sqb_skip(const sqb_eval_t &a, const sqb_inst_t &I, long c){
     if(a.skip) return a.skip[c];
     if(a.flag_at >= 0 && a.abskip){
-        int fl = a.esize == 1 ? ((const signed char*)a.pts)[c*(long)a.stride + a.flag_at]
-                              : ((const short*)a.pts)[c*(long)a.stride + a.flag_at];
+        int fl = a.esize == 1 ? ((const signed char*)I.pts)[c*(long)a.stride + a.flag_at]
+                              : ((const short*)I.pts)[c*(long)a.stride + a.flag_at];
         return fl & 1;
     }
     return 0;
 }
 
-__device__ __forceinline__ void sqb_tables(const sqb_eval_t &a, double *sX, double *sW){
-    const int nt = 2*a.K + 1;
-    for(int j = threadIdx.x; j < nt; j += blockDim.x){ sX[j] = a.X[j]; sW[j] = a.Wt ? a.Wt[j] : a.X[j]*a.H; }
+/* the launch's tables into shared memory (X then the weight factor Wt = X H when a batch has no Wt) and
+ * the integral records: one batch (ninst = 0) fills sI[0] */
+__device__ __forceinline__ void sqb_tables(const sqb_eval_t &a, double *sm, sqb_inst_t *sI){
+    if(a.ninst <= 0){
+        const int nt = 2*a.K + 1;
+        for(int j = threadIdx.x; j < nt; j += blockDim.x){ sm[j] = a.X[j]; sm[nt + j] = a.Wt ? a.Wt[j] : a.X[j]*a.H; }
+        if(threadIdx.x == 0) sqb_inst_of(a, &sI[0]);
+    } else {
+        for(int q = 0; q < a.ninst; q++){
+            const sqb_inst_t &I = a.inst[q];
+            const int nt = 2*I.K + 1;
+            for(int j = threadIdx.x; j < nt; j += blockDim.x){ sm[I.toff + j] = I.X[j]; sm[I.toff + nt + j] = I.Wt[j]; }
+        }
+        if(threadIdx.x < a.ninst) sI[threadIdx.x] = a.inst[threadIdx.x];
+    }
     __syncthreads();
 }
 
@@ -117,16 +153,16 @@ __device__ __forceinline__ void sqb_tables(const sqb_eval_t &a, double *sX, doub
  * of point i: skipped points keep fw; otherwise the bound abw 16 eps / DDSLACK sets the near flag and,
  * above ABSERR, queues the point for the double-double pass (value 0 until then).  Writes v[i] and
  * stt[i]; returns the value */
-__device__ __forceinline__ double sqb_point_test(const sqb_eval_t &a, long i, int sk, bool noab, double fw, double abw,
-                                                 bool *fallback){
+__device__ __forceinline__ double sqb_point_test(const sqb_eval_t &a, const sqb_inst_t &I, long i, int sk, bool noab,
+                                                 double fw, double abw, bool *fallback){
     unsigned char s = SQB_PRESENT | (sk ? SQB_SKIPPED : 0);
     double v;
     *fallback = false;
     if(noab) v = isfinite(fw) ? fw : 0.0;
     else {
         const double bnd = abw*16*DBL_EPSILON/a.ddslack;
-        if(!(bnd <= a.near_thr)) s |= SQB_NEAR;
-        if(!(bnd <= a.abserr)){
+        if(!(bnd <= I.near_thr)) s |= SQB_NEAR;
+        if(!(bnd <= I.abserr)){
             s |= SQB_FALLBACK; v = 0.0; *fallback = true;
             const unsigned long long q = atomicAdd(a.nfb, 1ULL);
             if((long)q < a.fbcap) a.fb[q] = i;
@@ -178,54 +214,72 @@ __device__ __forceinline__ void sqb_tile_flush(const sqb_eval_t &a, sqb_tile_acc
     }
 }
 
-/* The FP64 pass.  The CTAs take tiles of consecutive points in turn (tile b, b + gridDim.x, ...): SQB_TILE
- * points in level mode, SQB_BLOCK otherwise; in a tile, thread t evaluates points t, t + SQB_BLOCK, ...
- * (consecutive threads, consecutive points).
- * In level mode (a.part) each CTA also sums its tiles: the children that need no fallback add v*pw and
- * the rest into the thread's column of shared memory; a tile with a fallback point is only flagged
- * (a.tfb), and the reduce kernel sums it after the double-double pass. */
+/* The FP64 pass.  The CTAs take tiles of consecutive points in turn: tile b, b + gridDim.x, ... of one
+ * batch, or, in a multi-instance launch, the next tile of the device counter queue (the tile's integral
+ * from its position); SQB_TILE points per tile in level mode and in multi-instance launches, SQB_BLOCK
+ * otherwise.  In a tile, thread t evaluates points t, t + SQB_BLOCK, ... (consecutive threads, consecutive
+ * points).
+ * In level mode (a.part) each CTA also sums the tiles of its integrals that it is asked to (sqb_inst_t
+ * fused): the children that need no fallback add v*pw and the rest into the thread's column of shared
+ * memory; a tile with a fallback point, or of an integral the reduce kernel sums, is only flagged (a.tfb),
+ * and the reduce kernel sums it after the double-double pass. */
 template<class F, int D>
-__global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const sqb_eval_t a){
+__global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_constant__ sqb_eval_t a){
     extern __shared__ double sqb_sm[];
-    double *sX = sqb_sm, *sW = sqb_sm + (2*a.K + 1);
+    __shared__ sqb_inst_t sI[SQB_MAXINST];
+    __shared__ long s_tile;
+    __shared__ int s_k;
 #if SQB_FUSE
     __shared__ sqb_tile_acc ta;
     const bool lvl = a.part != NULL;
 #else
     const bool lvl = false;
 #endif
-    sqb_tables(a, sX, sW);
-    const long n = a.cells ? (a.n << D) : a.n;
-    const long tl = lvl ? SQB_TILE : SQB_BLOCK;          /* other modes: one point per thread per step */
-    const long ntiles = (n + tl - 1)/tl;
+    sqb_tables(a, sqb_sm, sI);
+    const bool multi = a.ninst > 0;
+    const long n1 = multi ? 0 : (a.cells ? (a.n << D) : a.n);      /* one batch: its points */
+    const long tl = (lvl || multi) ? SQB_TILE : SQB_BLOCK;          /* other modes: one point per thread per step */
+    const long ntiles = multi ? a.ntile : (n1 + tl - 1)/tl;
     const int t = threadIdx.x;
-    for(long tile = blockIdx.x; tile < ntiles; tile += gridDim.x){
+    long tile = blockIdx.x;
+    if(multi){ if(t == 0) s_tile = (long)atomicAdd(a.queue, 1ULL); __syncthreads(); tile = s_tile; }
+    while(tile < ntiles){
+        int k = 0;
+        if(multi){ if(t == 0) s_k = sqb_inst_at(a, tile*tl); __syncthreads(); k = s_k; }
+        const sqb_inst_t &I = sI[k];
+        const double *sX = sqb_sm + I.toff, *sW = sX + (2*I.K + 1);
+        const long base = multi ? tile*tl - I.child0 : tile*tl;     /* the tile's first point in its integral */
+        const long n = multi ? (a.cells ? (I.n << D) : I.n) : n1;
+        const long off = multi ? I.child0 : 0;                       /* global index = local index + off */
 #if SQB_FUSE
-        if(lvl){
+        const bool tsum = lvl && I.fused;
+        if(tsum){
             ta.S[0][t] = ta.S[1][t] = ta.A[t] = ta.dr[t] = ta.b1[0][t] = ta.b1[1][t] = ta.b2[0][t] = ta.b2[1][t] = 0;
             ta.ne[t] = ta.nsk[t] = ta.keep[t] = 0;
             if(t == 0) ta.fb = 0;
             __syncthreads();
         }
+#else
+        const bool tsum = false;
 #endif
         for(int j = 0; j < tl/SQB_BLOCK; j++){
-            const long i = tile*tl + (long)j*SQB_BLOCK + t;
+            const long il = base + (long)j*SQB_BLOCK + t, i = il + off;
             long c = 0; double sf[D], w = 0;
             int mw = 0, sk = 1;
             if constexpr(F::lockstep){
                 /* every thread of the block evaluates, a point outside the batch or not a point at a
                  * stand-in node (s = 1, discarded), and the |.| sums are evaluated when any thread of the
                  * block needs them (the value f does not depend on that choice) */
-                if(tile*tl + (long)j*SQB_BLOCK >= n) break;          /* the same for the whole block */
-                if(i < n) mw = sqb_point<D>(a, sX, sW, i, &c, sf, &w);
+                if(base + (long)j*SQB_BLOCK >= n) break;             /* the same for the whole block */
+                if(il < n) mw = sqb_point<D>(a, I, sX, sW, il, i, &c, sf, &w);
                 if(!mw){
 #pragma unroll
                     for(int d = 0; d < D; d++) sf[d] = 1.0;
-                } else sk = sqb_skip<D>(a, c);
+                } else sk = sqb_skip<D>(a, I, c);
             } else {
-                if(i >= n) break;
-                mw = sqb_point<D>(a, sX, sW, i, &c, sf, &w);
-                if(mw) sk = sqb_skip<D>(a, c);
+                if(il >= n) break;
+                mw = sqb_point<D>(a, I, sX, sW, il, i, &c, sf, &w);
+                if(mw) sk = sqb_skip<D>(a, I, c);
             }
             const bool noab = sk && !a.abcheck;
             double ab = 0, f = 0;
@@ -237,56 +291,69 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const sqb_eval_
                 else     f = F::template f<double, 1>(sf, &ab);
             }
             if(!mw){
-                if(i < n){ a.v[i] = 0; if(a.raw) a.ab[i] = 0; else a.stt[i] = 0; }
+                if(il < n){ a.v[i] = 0; if(a.raw) a.ab[i] = 0; else a.stt[i] = 0; }
                 continue;
             }
             if(noab) ab = 0;
             const double fw = f*w;
             if(a.raw){ a.v[i] = fw; a.ab[i] = ab*w; continue; }
             bool fallback;
-            const double v = sqb_point_test(a, i, sk, noab, fw, ab*w, &fallback);
+            const double v = sqb_point_test(a, I, i, sk, noab, fw, ab*w, &fallback);
 #if SQB_FUSE
-            if(lvl){
+            if(tsum){
                 if(fallback){ ta.fb = 1; continue; }
                 /* a folded point stands for its orbit: (mw v) pw and mw |v| (driver/sum.c:734-745) */
-                const double m = (double)mw, vp = (m*v)*a.pw, av = fabs(v);
+                const double m = (double)mw, vp = (m*v)*I.pw, av = fabs(v);
                 sqb_acc_dd(ta.S, t, vp); ta.A[t] += m*av; ta.ne[t]++; ta.nsk[t] += sk ? 1 : 0;
-                if(a.last){
+                if(I.last){
                     const int te = a.cfl ? (a.cfl[i] >> 1) & 3
-                                         : (((const signed char*)a.pts)[c*(long)a.stride + a.flag_at] >> 1) & 3;
+                                         : (((const signed char*)I.pts)[c*(long)a.stride + a.flag_at] >> 1) & 3;
                     if(te >= 1) sqb_acc_dd(ta.b1, t, vp);
                     if(te >= 2) sqb_acc_dd(ta.b2, t, vp);
-                } else if(av >= a.thr) ta.keep[t] += mw;
-                else ta.dr[t] += (m*av)*a.pw;
+                } else if(av >= I.thr) ta.keep[t] += mw;
+                else ta.dr[t] += (m*av)*I.pw;
             }
 #else
             (void)fallback;
 #endif
         }
 #if SQB_FUSE
-        if(lvl){
+        if(tsum){
             __syncthreads();
             if(ta.fb){ if(t == 0) a.tfb[tile] = 1; }
             else sqb_tile_flush(a, ta, tile);
             __syncthreads();
-        }
+        } else
 #endif
+        if(multi && a.tfb && t == 0) a.tfb[tile] = 1;                /* summed by the reduce kernel */
+        if(multi){
+            __syncthreads();                                          /* every thread has read s_tile, s_k */
+            if(t == 0) s_tile = (long)atomicAdd(a.queue, 1ULL);
+            __syncthreads();
+            tile = s_tile;
+        } else tile += gridDim.x;
     }
 }
 
 template<class F, int D>
-__global__ void __launch_bounds__(SQB_BLOCK) sqb_k_dd(const sqb_dd_t a){
+__global__ void __launch_bounds__(SQB_BLOCK) sqb_k_dd(const __grid_constant__ sqb_dd_t a){
     extern __shared__ double sqb_sm[];
+    __shared__ sqb_inst_t sI[SQB_MAXINST];
     const sqb_eval_t &e = a.e;
-    double *sX = sqb_sm, *sW = sqb_sm + (2*e.K + 1);
-    sqb_tables(e, sX, sW);
+    sqb_tables(e, sqb_sm, sI);
+    const bool multi = e.ninst > 0;
     long n;
-    if(a.all) n = e.cells ? (e.n << D) : e.n;
+    if(a.all) n = multi ? e.ntile*SQB_TILE : (e.cells ? (e.n << D) : e.n);
     else { n = (long)*a.nlist; if(n > a.listcap) n = a.listcap; }
     for(long j = blockIdx.x*(long)blockDim.x + threadIdx.x; j < n; j += (long)gridDim.x*blockDim.x){
         const long i = a.all ? j : a.list[j];
+        const int k = multi ? sqb_inst_at(e, i) : 0;
+        const sqb_inst_t &I = sI[k];
+        const double *sX = sqb_sm + I.toff, *sW = sX + (2*I.K + 1);
+        const long il = i - I.child0;
+        if(multi && il >= (e.cells ? (I.n << D) : I.n)) continue;    /* a tile's padding: no point */
         long c; double sf[D], w;
-        if(!sqb_point<D>(e, sX, sW, i, &c, sf, &w)){ e.v[i] = 0; e.stt[i] = 0; a.uu[i] = 0; continue; }
+        if(!sqb_point<D>(e, I, sX, sW, il, i, &c, sf, &w)){ e.v[i] = 0; e.stt[i] = 0; a.uu[i] = 0; continue; }
         sqdd sq[D], abq;
 #pragma unroll
         for(int d = 0; d < D; d++) sq[d] = sqdd(sf[d]);
@@ -295,13 +362,13 @@ __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_dd(const sqb_dd_t a){
         const double vqd = vq.value(), abqd = abq.value();
         /* qvalue(), driver/eval.c:25-30 */
         const double ee = abqd*w*SQB_QEPS;
-        const double u = !(ee*16 <= e.abserr) ? (isfinite(ee) ? ee*ee : 0.0) : 0.0;
+        const double u = !(ee*16 <= I.abserr) ? (isfinite(ee) ? ee*ee : 0.0) : 0.0;
         double v = isfinite(vqd) ? vqd*w : 0.0;
         unsigned char s;
         if(a.all){
             /* the all-double-double form: the near flag from the double-double |.| sum */
-            s = SQB_PRESENT | SQB_FALLBACK | (sqb_skip<D>(e, c) ? SQB_SKIPPED : 0);
-            if(!(abqd*w*16*DBL_EPSILON/e.ddslack <= e.near_thr)) s |= SQB_NEAR;
+            s = SQB_PRESENT | SQB_FALLBACK | (sqb_skip<D>(e, I, c) ? SQB_SKIPPED : 0);
+            if(!(abqd*w*16*DBL_EPSILON/e.ddslack <= I.near_thr)) s |= SQB_NEAR;
         } else s = e.stt[i];
         if(!(ee <= fabs(v))){ s |= SQB_UNRES; if(a.dropunres) v = 0.0; }
         e.v[i] = v; e.stt[i] = s; a.uu[i] = u;
@@ -317,13 +384,15 @@ __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_dd(const sqb_dd_t a){
 template<class F, int D, int P>
 __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_part(const sqb_eval_t a, double *tt, double *ta){
     extern __shared__ double sqb_sm[];
-    double *sX = sqb_sm, *sW = sqb_sm + (2*a.K + 1);
-    sqb_tables(a, sX, sW);
+    __shared__ sqb_inst_t sI[1];
+    sqb_tables(a, sqb_sm, sI);                       /* one batch (ninst = 0) */
+    const sqb_inst_t &I = sI[0];
+    const double *sX = sqb_sm, *sW = sqb_sm + (2*a.K + 1);
     const long n = a.cells ? (a.n << D) : a.n;
     for(long i = blockIdx.x*(long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x*blockDim.x){
         long c; double sf[D], w;
-        if(!sqb_point<D>(a, sX, sW, i, &c, sf, &w)) continue;
-        const int sk = sqb_skip<D>(a, c);
+        if(!sqb_point<D>(a, I, sX, sW, i, i, &c, sf, &w)) continue;
+        const int sk = sqb_skip<D>(a, I, c);
         double T = P ? tt[i] : 0.0, A = P ? ta[i] : 0.0;
         if(sk && !a.abcheck) F::template part<P, 0>(sf, &T, &A);
         else                 F::template part<P, 1>(sf, &T, &A);
@@ -334,19 +403,21 @@ __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_part(const sqb_eval_t a, doub
 template<class F, int D>
 __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_fin(const sqb_eval_t a, const double *tt, const double *ta){
     extern __shared__ double sqb_sm[];
-    double *sX = sqb_sm, *sW = sqb_sm + (2*a.K + 1);
-    sqb_tables(a, sX, sW);
+    __shared__ sqb_inst_t sI[1];
+    sqb_tables(a, sqb_sm, sI);                       /* one batch (ninst = 0) */
+    const sqb_inst_t &I = sI[0];
+    const double *sX = sqb_sm, *sW = sqb_sm + (2*a.K + 1);
     const long n = a.cells ? (a.n << D) : a.n;
     for(long i = blockIdx.x*(long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x*blockDim.x){
         long c; double sf[D], w;
-        if(!sqb_point<D>(a, sX, sW, i, &c, sf, &w)){ a.v[i] = 0; a.stt[i] = 0; continue; }
-        const int sk = sqb_skip<D>(a, c);
+        if(!sqb_point<D>(a, I, sX, sW, i, i, &c, sf, &w)){ a.v[i] = 0; a.stt[i] = 0; continue; }
+        const int sk = sqb_skip<D>(a, I, c);
         const bool noab = sk && !a.abcheck;
         double ab = 0, f;
         if(noab) f = F::template fin<0>(sf, tt[i], ta[i], &ab);
         else     f = F::template fin<1>(sf, tt[i], ta[i], &ab);
         bool fallback;
-        sqb_point_test(a, i, sk, noab, f*w, ab*w, &fallback);
+        sqb_point_test(a, I, i, sk, noab, f*w, ab*w, &fallback);
     }
 }
 

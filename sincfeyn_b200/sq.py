@@ -24,7 +24,7 @@ class Opts(C.Structure):
                 ('abskip', C.c_int), ('abcheck', C.c_int), ('dropunres', C.c_int), ('growskip', C.c_int),
                 ('alldd', C.c_int), ('device', C.c_int), ('max_children', C.c_long), ('verbose', C.c_int),
                 ('ckpt_every', C.c_double), ('ckpt_dir', C.c_char_p), ('ckpt_stop', C.c_int), ('fma', C.c_int),
-                ('split', C.c_int), ('sym', C.c_char_p), ('predict', C.c_double)]
+                ('split', C.c_int), ('sym', C.c_char_p), ('predict', C.c_double), ('group', C.c_int)]
 
 
 class Result(C.Structure):
@@ -243,6 +243,23 @@ def hsum_batch(jobs, workers=4, **opts):
     if rc:
         raise SqbError('batch: %d failed: %s' % (rc, lib().sqb_error().decode()))
     return [_result_dict(res[i]) for i in range(n)], ms.value
+
+
+def hsum_group(jobs, **opts):
+    """Several integrals of one graph as one group (sqb_hsum_group): jobs = [(graph, h, N, eps[, top])], at
+    most 8, all of the same graph; their refinement levels run as shared launches.  Returns the results
+    in job order as hsum() dicts (each bit for bit the hsum() result)."""
+    arr = _jobs(jobs)
+    n = len(jobs)
+    res = (Result * max(1, n))()
+    rcs = (C.c_int * max(1, n))()
+    o = default_opts(**opts)
+    L = lib()
+    L.sqb_hsum_group.argtypes = [C.POINTER(Job), C.c_int, C.POINTER(Opts), C.POINTER(Result), C.POINTER(C.c_int)]
+    rc = L.sqb_hsum_group(arr, n, C.byref(o), res, rcs)
+    if rc:
+        raise SqbError('group: %d failed: %s' % (rc, L.sqb_error().decode()))
+    return [_result_dict(res[i]) for i in range(n)]
 
 
 def batch_tune(jobs, candidates=(1, 2, 4, 6, 8), **opts):

@@ -32,12 +32,15 @@ Fixtures
                                 (`run 2.0 13 1e-4 GRAPH`, SINCQED_SYM unset = auto; the search's nodes only
                                 need K >= 6), and folded sums (SINCQED_SYM unset, SINCQED_KEEPBT=1) with
                                 top = 2 so that kept orbits go on to a second refinement level
+  all2_mixed_h.json             all2 at h = 1.0, 0.9, 0.8, 0.7 (N = 2 ceil(48/h) + 1, eps = 1e-12), the
+                                -ffp-contract=off build with SINCQED_SYM=0 and SINCQED_KEEPBT=1: the two-loop
+                                part of the mixed batch
   all3_h0.7_N139_eps1e-12.json  `sincqed run 0.7 139 1e-12 GRAPH` for the 41 three-loop integrals (the headline
                                 workload), -ffp-contract=off build, SINCQED_SYM=0, SINCQED_KEEPBT=1, default
                                 top = 2: every results column, the fallback count and the host wall time
                                 (an hour or more on 8 cores; resumable, see all3())
 
-    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold scale predict all3]
+    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold scale predict all3 mixed2]
     (default: all but all3)
 """
 import json
@@ -193,6 +196,25 @@ def fold():
         json.dump(d, f, indent=1)
 
 
+MIX_H = (1.0, 0.9, 0.8, 0.7)
+
+
+def mixed2():
+    """all2 at each h of the mixed batch (N = 2 ceil(48/h) + 1, eps = 1e-12, default top): the
+    -ffp-contract=off build, SINCQED_SYM=0, SINCQED_KEEPBT=1"""
+    import math
+    d = {'env': {'SINCQED_SYM': '0', 'SINCQED_KEEPBT': '1'}, 'eps': 1e-12, 'runs': []}
+    for h in MIX_H:
+        N = 2*math.ceil(48/h - 1e-9) + 1
+        rows, out = refpy.run(refpy.SINCQED_EXACT, h, N, 1e-12, ['all2'], env=d['env'])
+        for r in with_log(rows, out):
+            r.pop('time_s', None)
+            r.update(h=h, N=N)
+            d['runs'].append(r)
+    with open(os.path.join(OUT, 'all2_mixed_h.json'), 'w') as f:
+        json.dump(d, f, indent=1)
+
+
 ALL3 = (0.7, 139, 1e-12)
 ALL3_FILE = os.path.join(OUT, 'all3_h0.7_N139_eps1e-12.json')
 
@@ -253,6 +275,8 @@ if __name__ == '__main__':
     parts = sys.argv[1:] or ['all2', 'boxsum', 'pointwise', 'synth', 'fold', 'scale', 'predict']
     if 'all3' in parts:
         all3()
+    if 'mixed2' in parts:
+        mixed2()
     if 'all2' in parts:
         all2()
     if 'boxsum' in parts:

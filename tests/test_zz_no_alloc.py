@@ -33,7 +33,8 @@ class Level(C.Structure):
     _fields_ = [('g', C.c_void_p), ('cells', C.c_void_p), ('ncell', C.c_long), ('next', C.c_void_p),
                 ('next_cap', C.c_long), ('st', C.c_int), ('last', C.c_int), ('pw', C.c_double), ('thr', C.c_double),
                 ('t', PointTestParams), ('max_children', C.c_long), ('sym', C.c_void_p), ('vt', C.c_void_p),
-                ('vput', C.c_int), ('predict', C.c_double), ('esok', C.c_int)]
+                ('vput', C.c_int), ('predict', C.c_double), ('esok', C.c_int), ('X', C.c_void_p), ('Wt', C.c_void_p),
+                ('K', C.c_int)]
 
 
 class Acc(C.Structure):
