@@ -406,8 +406,8 @@ def main():
     ap.add_argument('--graph', default='g3_00', help='--workload single/points: the graph')
     ap.add_argument('--prec', type=int, default=2, help='--workload points: 0 FP64 as written, 2 contracted, 1 dd')
     ap.add_argument('--npoints', type=int, default=1 << 22, help='--workload points: number of nodes')
-    ap.add_argument('--split', type=int, default=0, help='--workload single: the FP64 pass form of a graph with '
-                    'node passes (0 one kernel, 1 passes, 2 lockstep)')
+    ap.add_argument('--split', type=int, default=0, help='--workload single: 1 = the FP64 pass of a graph with '
+                    'node passes in passes (0: one kernel)')
     ap.add_argument('--h', type=float, default=0.0, help='--workload single: h (default 0.7)')
     ap.add_argument('--N', type=int, default=0, help='--workload single: N (default 2ceil(48/h)+1)')
     ap.add_argument('--workload', default='all3', choices=['all3', 'mixed', 'synth', 'vp4', 'single', 'points'],

@@ -80,11 +80,10 @@ typedef struct {
                               and adds fused, as the reference's own CPU build compiles its double half);
                               0 = the kernel that rounds every operation as written, bit for bit the reference's
                               double half built with -ffp-contract=off */
-    int split;             /* SQB_SPLIT, the FP64 pass of the level batches of a graph whose point function is a
-                              flat sum of independent forest nodes (g3_lbl): 0 (default) = one kernel;
-                              1 = passes over groups of nodes (the same operations in the same order: the same
-                              values); 2 = one contracted kernel in lockstep, the threads of a block meeting at
-                              the start of every node so that its warps share the fetched instructions */
+    int split;             /* SQB_SPLIT: 1 = a graph whose point function is a flat sum of independent forest
+                              nodes (g3_lbl) runs the FP64 pass of its level batches as passes over groups of
+                              nodes (the same operations in the same order: the same values); 0 (default) = one
+                              pass, measured faster on the B200 */
     const char *sym;       /* SINCQED_SYM, the symmetry fold (driver/sum.c:21-26, 566-592): NULL, "0" or "off" = no
                               fold (the default, and the reference's GPU build, whose point set is the unfolded
                               tree); "auto" = find the group of axis permutations that leave the integrand

@@ -181,15 +181,6 @@ def split_plan(k, max_parts=12):
     return groups, '\n'.join(out)
 
 
-def lockstep_markers(body, name):
-    """SQ_NODE_SYNC(SQ_LS); before every `/* node` section of the point function pt_<name> in body"""
-    head = 'FN(pt_%s)(const REAL *x, const REAL Vx, REAL *ab){' % name
-    i = body.index(head)
-    j = body.index('\n}\n', i)
-    seg = re.sub(r'^(\s*)(/\* node)', r'\1SQ_NODE_SYNC(SQ_LS);\n\1\2', body[i:j], flags=re.M)
-    return body[:i] + seg + body[j:]
-
-
 def emit(src):
     """Header text for one graph: namespace SQG_NS(<name>) (a macro of the including unit, normally
     sqg_<name>) with the tables and two copies of the class
@@ -204,16 +195,9 @@ def emit(src):
     for name, n, vals in k.gl:
         out.append('SQ_TABLE double %s[%d] = {%s};' % (name, n, vals))
     plan = split_plan(k)
-    body = k.body('SQ_CHUNK', 'SQ_FUNC_K').strip('\n')
-    if plan:
-        # a graph made of independent forest nodes also gets a lockstep form (K<.., SQ_LS = 1>): the threads
-        # of a block meet at the start of every node (SQ_NODE_SYNC), so that its warps run the same code at
-        # the same time and share what the instruction caches fetch
-        body = lockstep_markers(body, k.name)
-        out += ['#ifndef SQ_NODE_SYNC', '#define SQ_NODE_SYNC(ls) ((void)0)', '#endif']
     out += ['#define REAL SqReal_', '#define FN(x) x',
-            'template<class SqReal_, int SQ_AB%s> struct K {' % (', int SQ_LS = 0' if plan else ''),
-            body]
+            'template<class SqReal_, int SQ_AB> struct K {',
+            k.body('SQ_CHUNK', 'SQ_FUNC_K').strip('\n')]
     if plan:
         out += ['/* the same point function in %d passes over groups of its nodes (kgen.split_plan) */' % len(plan[0]),
                 plan[1]]

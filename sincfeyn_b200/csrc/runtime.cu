@@ -214,11 +214,7 @@ static void fill_eval(sqb_eval_t *a, const sqb_test_t *t){
 
 /* whether a batch's FP64 pass runs in passes (the graph has them, they are asked for, a level batch) */
 static inline bool use_split(const sqb_graph_t *g, const sqb_eval_t *a, const sqb_test_t *t){
-    return t->split == 1 && g->nparts > 0 && a->cells && !t->alldd;
-}
-/* whether a level batch's FP64 pass runs the graph's lockstep kernel (split = 2, contracted form) */
-static inline bool use_lockstep(const sqb_graph_t *g, const sqb_eval_t *a, const sqb_test_t *t){
-    return t->split == 2 && t->fma && g->f64_ls && g->attr_ls && a->cells && !t->alldd;
+    return t->split && g->nparts > 0 && a->cells && !t->alldd;
 }
 
 /* FP64 pass (or the all-dd pass) and the fallback pass for one batch already described by a */
@@ -259,13 +255,6 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
             CKR(cudaGetLastError());
         }
         G.launches += g->nparts;
-    } else if(use_lockstep(g, a, t)){
-        sqb_kattr_t at; memset(&at, 0, sizeof at); int per = 2;
-        if(g->attr_ls(128, smem, &at) && at.blocks_per_sm > 0) per = at.blocks_per_sm;
-        const long want = a->ninst > 0 ? a->ntile : (npts + 127)/128, full = (long)G.nsm*per;
-        if(a->ninst > 0) CKR(cudaMemsetAsync(a->queue, 0, sizeof(unsigned long long), G.s));
-        g->f64_ls(a, (int)(want < full ? want : full), 128, smem, G.s);
-        CKR(cudaGetLastError());
     } else {
         const int w = f64_which(g, t->fma);
         if(a->ninst > 0){
@@ -644,8 +633,7 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
          * pass: the reduce kernel sums every tile) */
         int can = 0;
         const long cap = grid_cap(g, f64_which(g, L->t.fma), 2*(2*G.K + 1)*sizeof(double), &can);
-        const bool fused = !L->t.alldd && can && !use_split(g, &a, &L->t) && !use_lockstep(g, &a, &L->t) &&
-                           nch >= 2*SQB_TILE*cap;
+        const bool fused = !L->t.alldd && can && !use_split(g, &a, &L->t) && nch >= 2*SQB_TILE*cap;
         /* the predictor at the last level: which children to leave out, and their tiers */
         if(pon){
             if(sqb_vtab_predict(L->vt, cells, nc, D, L->st, G.K, L->thr, L->predict, L->esok, L->sym, G.cfl,
@@ -700,7 +688,7 @@ extern "C" int sqb_dev_level_multi(const sqb_level_t *Ls, int n, sqb_acc_t *accs
     const sqb_graph_t *g = Ls[0].g; const int D = g->D;
     for(int k = 0; k < n && !one_by_one; k++){
         const sqb_level_t &L = Ls[k];
-        one_by_one = L.g != g || L.t.alldd || L.t.split == 1 || L.predict > 0 || L.vput || L.st != Ls[0].st ||
+        one_by_one = L.g != g || L.t.alldd || L.t.split || L.predict > 0 || L.vput || L.st != Ls[0].st ||
                      L.last != Ls[0].last || !L.X || !L.Wt || L.K < 1 || L.K > 127 || L.t.fma != Ls[0].t.fma ||
                      L.t.split != Ls[0].t.split || L.t.abskip != Ls[0].t.abskip || L.t.abcheck != Ls[0].t.abcheck ||
                      L.t.dropunres != Ls[0].t.dropunres || L.t.ddslack != Ls[0].t.ddslack ||
@@ -771,7 +759,7 @@ extern "C" int sqb_dev_level_multi(const sqb_level_t *Ls, int n, sqb_acc_t *accs
             const long c0 = r*ncb[k], nc = L.ncell - c0 < ncb[k] ? L.ncell - c0 : ncb[k], nch = nc << D;
             sqb_inst_t &I = a.inst[m];
             I.pts = L.cells + c0; I.n = nc; I.child0 = child0; I.st = L.st; I.K = L.K; I.toff = toff;
-            I.fused = cank[k] && !use_lockstep(g, &a, &L.t) && nch >= 2*SQB_TILE*capk[k];
+            I.fused = cank[k] && nch >= 2*SQB_TILE*capk[k];
             I.last = L.last; I.pw = L.pw; I.thr = L.thr; I.abserr = L.t.abserr; I.near_thr = L.t.nearf*L.t.abserr;
             I.X = L.X; I.Wt = L.Wt;
             lvi_t &V = rl.inst[m];

@@ -144,10 +144,6 @@ typedef struct {
     int (*split_attr)(int P, int fma, int block, size_t smem, sqb_kattr_t *out);
     /* the scaling test on the raw double-double point function ptq; NULL for graphs without one (VP) */
     void (*scale)(const sqb_scale_t *a, int grid, int block, void *stream);
-    /* graphs with passes (nparts > 0): the contracted FP64 kernel in lockstep, its block's threads meeting at
-     * every forest node so that they share fetched instructions; NULL if not in the library */
-    void (*f64_ls)(const sqb_eval_t *a, int grid, int block, size_t smem, void *stream);
-    int (*attr_ls)(int block, size_t smem, sqb_kattr_t *out);
 } sqb_graph_t;
 
 #ifdef __cplusplus

@@ -36,11 +36,6 @@
 #define RABS(x) sq_rabs(x)
 #define SQ_EXP(x) sq_exp(x)
 #define SQ_LOG(x) sq_log(x)
-/* the lockstep form of a graph made of independent forest nodes (kgen: K<.., .., SQ_LS = 1>): every thread
- * of the block meets the others at the start of each node, so that the block's warps run the same code
- * together and share what the instruction caches fetch (the kernel guarantees that every thread of the
- * block calls the point function the same number of times) */
-#define SQ_NODE_SYNC(ls) do { if constexpr((ls) != 0) __syncthreads(); } while(0)
 
 #ifndef SQB_BLOCK
 #define SQB_BLOCK 128
@@ -264,37 +259,19 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
 #endif
         for(int j = 0; j < tl/SQB_BLOCK; j++){
             const long il = base + (long)j*SQB_BLOCK + t, i = il + off;
-            long c = 0; double sf[D], w = 0;
-            int mw = 0, sk = 1;
-            if constexpr(F::lockstep){
-                /* every thread of the block evaluates, a point outside the batch or not a point at a
-                 * stand-in node (s = 1, discarded), and the |.| sums are evaluated when any thread of the
-                 * block needs them (the value f does not depend on that choice) */
-                if(base + (long)j*SQB_BLOCK >= n) break;             /* the same for the whole block */
-                if(il < n) mw = sqb_point<D>(a, I, sX, sW, il, i, &c, sf, &w);
-                if(!mw){
-#pragma unroll
-                    for(int d = 0; d < D; d++) sf[d] = 1.0;
-                } else sk = sqb_skip<D>(a, I, c);
-            } else {
-                if(il >= n) break;
-                mw = sqb_point<D>(a, I, sX, sW, il, i, &c, sf, &w);
-                if(mw) sk = sqb_skip<D>(a, I, c);
-            }
-            const bool noab = sk && !a.abcheck;
-            double ab = 0, f = 0;
-            if constexpr(F::lockstep){
-                if(__syncthreads_or(mw && !noab)) f = F::template f<double, 1>(sf, &ab);
-                else                              f = F::template f<double, 0>(sf, &ab);
-            } else if(mw){
-                if(noab) f = F::template f<double, 0>(sf, &ab);
-                else     f = F::template f<double, 1>(sf, &ab);
-            }
+            if(il >= n) break;
+            long c; double sf[D], w;
+            const int mw = sqb_point<D>(a, I, sX, sW, il, i, &c, sf, &w);
             if(!mw){
-                if(il < n){ a.v[i] = 0; if(a.raw) a.ab[i] = 0; else a.stt[i] = 0; }
+                a.v[i] = 0;
+                if(a.raw) a.ab[i] = 0; else a.stt[i] = 0;
                 continue;
             }
-            if(noab) ab = 0;
+            const int sk = sqb_skip<D>(a, I, c);
+            const bool noab = sk && !a.abcheck;
+            double ab = 0, f;
+            if(noab) f = F::template f<double, 0>(sf, &ab);
+            else     f = F::template f<double, 1>(sf, &ab);
             const double fw = f*w;
             if(a.raw){ a.v[i] = fw; a.ab[i] = ab*w; continue; }
             bool fallback;
@@ -468,11 +445,6 @@ __global__ void __launch_bounds__(SQB_BLOCK) sqb_k_scale(const sqb_scale_t a){
 /* the split form's point functions (SQ_GRAPH_SPLIT): pass P and the final pass in FP64 */
 #define SQ_SPLIT_F(NAME)                                                                           \
 namespace SQG_NS(NAME) {                                                                           \
-struct FL {                                                                                        \
-    static constexpr bool lockstep = true;                                                         \
-    template<class R, int AB> static __device__ __forceinline__ R f(const R *sf, R *ab){           \
-        return K<R, AB, 1>::f_##NAME(sf, ab); }                                                    \
-};                                                                                                 \
 struct FS {                                                                                        \
     template<int P, int AB> static __device__ __forceinline__ void part(const double *sf, double *T, double *A){ \
         K<double, AB>::template fpart_##NAME<P>(sf, T, A); }                                       \
@@ -485,7 +457,6 @@ struct FS {                                                                     
 #define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
 namespace SQG_NS(NAME) {                                                                           \
 struct F {                                                                                         \
-    static constexpr bool lockstep = false;                                                        \
     template<class R, int AB> static __device__ __forceinline__ R f(const R *sf, R *ab){           \
         return K<R, AB>::f_##NAME(sf, ab); }                                                       \
 };                                                                                                 \
@@ -506,11 +477,7 @@ extern "C" void SQB_##NAME##_splitfma(int P, const sqb_eval_t *a, double *tt, do
                                       size_t smem, void *st){                                      \
     sqb_split_launch<SQG_NS(NAME)::FS, D, NPARTS>(P, a, tt, ta, grid, block, smem, (cudaStream_t)st); } \
 extern "C" int SQB_##NAME##_splitattrfma(int P, int block, size_t smem, sqb_kattr_t *o){          \
-    return sqb_split_attr<SQG_NS(NAME)::FS, D, NPARTS>(P, block, smem, o); }                        \
-extern "C" void SQB_##NAME##_f64ls(const sqb_eval_t *a, int grid, int block, size_t smem, void *st){ \
-    sqb_k_f64<SQG_NS(NAME)::FL, D><<<grid, block, smem, (cudaStream_t)st>>>(*a); }                 \
-extern "C" int SQB_##NAME##_attrls(int block, size_t smem, sqb_kattr_t *o){                        \
-    return sqb_attr_of(sqb_k_f64<SQG_NS(NAME)::FL, D>, block, smem, o); }
+    return sqb_split_attr<SQG_NS(NAME)::FS, D, NPARTS>(P, block, smem, o); }
 #else
 /* SQ_SCALE(name) follows SQ_GRAPH for a graph with a raw point function: its scaling-test launcher */
 #define SQ_SCALE(NAME)                                                                              \
@@ -528,7 +495,6 @@ extern "C" void SQB_##NAME##_scale(const sqb_scale_t *, int, int, void *) __attr
 extern "C" int SQB_##NAME##_attrfma(int, size_t, sqb_kattr_t *) __attribute__((weak));             \
 namespace SQG_NS(NAME) {                                                                           \
 struct F {                                                                                         \
-    static constexpr bool lockstep = false;                                                        \
     template<class R, int AB> static __device__ __forceinline__ R f(const R *sf, R *ab){           \
         return K<R, AB>::f_##NAME(sf, ab); }                                                       \
 };                                                                                                 \
@@ -554,15 +520,13 @@ static int attr(int which, int block, size_t smem, sqb_kattr_t *o){             
 SQ_GRAPH_CORE(NAME, D)                                                                             \
 extern "C" const sqb_graph_t SQB_##NAME = {#NAME, VOLKOV, L, D, W, NP, FIX, 0,                     \
     SQG_NS(NAME)::f64, SQG_NS(NAME)::dd, SQG_NS(NAME)::attr, SQB_##NAME##_f64fma, 0, NULL, NULL,     \
-    SQB_##NAME##_scale, NULL, NULL};
+    SQB_##NAME##_scale};
 #define SQ_GRAPH_SPLIT(NAME, VOLKOV, L, D, W, NP, FIX, NPARTS)                                      \
 SQ_GRAPH_CORE(NAME, D)                                                                             \
 SQ_SPLIT_F(NAME)                                                                                   \
 extern "C" void SQB_##NAME##_splitfma(int, const sqb_eval_t *, double *, double *, int, int, size_t, void *) \
     __attribute__((weak));                                                                         \
 extern "C" int SQB_##NAME##_splitattrfma(int, int, size_t, sqb_kattr_t *) __attribute__((weak));   \
-extern "C" void SQB_##NAME##_f64ls(const sqb_eval_t *, int, int, size_t, void *) __attribute__((weak)); \
-extern "C" int SQB_##NAME##_attrls(int, size_t, sqb_kattr_t *) __attribute__((weak));              \
 namespace SQG_NS(NAME) {                                                                           \
 static void split(int P, int fma, const sqb_eval_t *a, double *tt, double *ta, int grid, int block, size_t smem, \
                   void *st){                                                                       \
@@ -574,5 +538,5 @@ static int split_attr(int P, int fma, int block, size_t smem, sqb_kattr_t *o){  
 }                                                                                                  \
 extern "C" const sqb_graph_t SQB_##NAME = {#NAME, VOLKOV, L, D, W, NP, FIX, 0,                     \
     SQG_NS(NAME)::f64, SQG_NS(NAME)::dd, SQG_NS(NAME)::attr, SQB_##NAME##_f64fma, NPARTS,           \
-    SQG_NS(NAME)::split, SQG_NS(NAME)::split_attr, SQB_##NAME##_scale, SQB_##NAME##_f64ls, SQB_##NAME##_attrls};
+    SQG_NS(NAME)::split, SQG_NS(NAME)::split_attr, SQB_##NAME##_scale};
 #endif

@@ -35,13 +35,17 @@ Fixtures
   all2_mixed_h.json             all2 at h = 1.0, 0.9, 0.8, 0.7 (N = 2 ceil(48/h) + 1, eps = 1e-12), the
                                 -ffp-contract=off build with SINCQED_SYM=0 and SINCQED_KEEPBT=1: the two-loop
                                 part of the mixed batch
+  vp4_sample.json               four-loop lepton-loop kernels (kernels/v4, kernels/w4), a sample of D = 6..9 with
+                                the sets I(a), I(b), I(c) of docs/LEPTON_LOOPS.md, at h = 1.0 (N = 97) and 0.9
+                                (N = 107), eps = 1e-12, -ffp-contract=off build, SINCQED_SYM=0, SINCQED_KEEPBT=1
+                                (hours on 8 cores; resumable, see vp4())
   all3_h0.7_N139_eps1e-12.json  `sincqed run 0.7 139 1e-12 GRAPH` for the 41 three-loop integrals (the headline
                                 workload), -ffp-contract=off build, SINCQED_SYM=0, SINCQED_KEEPBT=1, default
                                 top = 2: every results column, the fallback count and the host wall time
                                 (an hour or more on 8 cores; resumable, see all3())
 
-    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold scale predict all3 mixed2]
-    (default: all but all3)
+    python tests/golden/make_golden.py [all2 boxsum pointwise synth fold scale predict all3 mixed2 vp4]
+    (default: all but all3, mixed2 and vp4)
 """
 import json
 import os
@@ -215,6 +219,39 @@ def mixed2():
         json.dump(d, f, indent=1)
 
 
+VP4_H = ((1.0, 97), (0.9, 107))
+# a dimension-stratified sample of kernels/v4 and kernels/w4 (D = 6, 7, 8, 9; the cheapest D = 9 graph at
+# h = 2.0), and the lepton-loop sets I(a), I(b), I(c) of docs/LEPTON_LOOPS.md:5-17
+VP4_SAMPLE = ['w4_00Sc', 'v4_00', 'w4_00Sm', 'w4_00Vm', 'w4_0iSc', 'w4_0iSm', 'w4_0iVm', 'v4_02', 'v4_14']
+VP4_FILE = os.path.join(OUT, 'vp4_sample.json')
+
+
+def vp4():
+    """`sincqed run h N 1e-12 GRAPH` for VP4_SAMPLE at h = 1.0 (N = 97) and 0.9 (N = 107), default top = 1:
+    the -ffp-contract=off build, SINCQED_SYM=0, SINCQED_KEEPBT=1, one graph per process (checkpoints every
+    15 min; the file is rewritten after every run and runs already in it are kept)"""
+    d = {'env': {'SINCQED_SYM': '0', 'SINCQED_KEEPBT': '1'}, 'eps': 1e-12, 'threads': os.cpu_count(),
+         'cpu': _cpu_model(), 'runs': []}
+    if os.path.exists(VP4_FILE):
+        with open(VP4_FILE) as f:
+            d['runs'] = json.load(f)['runs']
+    done = {(r['name'], r['h']) for r in d['runs']}
+    ck = os.path.join(tempfile.gettempdir(), 'sincfeyn_golden_ckpt')
+    os.makedirs(ck, exist_ok=True)
+    for h, N in VP4_H:
+        for g in VP4_SAMPLE:
+            if (g, h) in done:
+                continue
+            env = dict(d['env'], SINCQED_CKPT='900', SINCQED_CKPT_DIR=ck)
+            rows, out = refpy.run(refpy.SINCQED_EXACT, h, N, 1e-12, [g], env=env, timeout=12*3600)
+            r = with_log(rows, out)[0]
+            r.update(h=h, N=N)
+            d['runs'].append(r)
+            with open(VP4_FILE, 'w') as f:
+                json.dump(d, f, indent=1)
+            print('%s h=%g %+.16e evals %d %.1f s' % (g, h, r['value'], r['evals'], r['time_s']), flush=True)
+
+
 ALL3 = (0.7, 139, 1e-12)
 ALL3_FILE = os.path.join(OUT, 'all3_h0.7_N139_eps1e-12.json')
 
@@ -277,6 +314,8 @@ if __name__ == '__main__':
         all3()
     if 'mixed2' in parts:
         mixed2()
+    if 'vp4' in parts:
+        vp4()
     if 'all2' in parts:
         all2()
     if 'boxsum' in parts:

@@ -1,15 +1,9 @@
-"""The FP64 pass of g3_lbl in its other forms (GPU).  g3_lbl's point function is a flat sum of twelve
-independent forest nodes.
-
-  * split = 1: its level batches run as passes over groups of nodes (one per main node, the zero-momentum
-    subtractions in pairs) and a final pass (kgen.split_plan).  Every operation and its order are those of
-    the single function, so with the as-written kernels the whole sum is bit for bit the single-pass one;
-    the contracted kernels may fuse differently inside a pass, so there the sums agree to the three-loop
-    tolerance.
-  * split = 2: one contracted kernel in lockstep (the threads of a block meet at the start of every node);
-    the same arithmetic as the single contracted kernel, every thread of a block evaluating (stand-in
-    nodes for threads without a point): the same evaluation count and the sum to the three-loop
-    tolerance."""
+"""The FP64 pass of g3_lbl in passes (GPU).  g3_lbl's point function is a flat sum of twelve independent
+forest nodes; with split = 1 its level batches run as passes over groups of nodes (one per main node, the
+zero-momentum subtractions in pairs) and a final pass (kgen.split_plan).  Every operation and its order are
+those of the single function, so with the as-written kernels the whole sum is bit for bit the single-pass
+one; the contracted kernels may fuse differently inside a pass, so there the sums agree to the three-loop
+tolerance."""
 import pytest
 
 from sincfeyn_b200 import sq
@@ -38,10 +32,3 @@ def test_split_contracted_within_tolerance():
     assert abs(many['nev'] - one['nev']) <= 1e-4*one['nev']
     assert abs(many['S'][0] - one['S'][0]) <= 1e-11*abs(one['S'][0])
 
-
-def test_lockstep_contracted_matches_the_single_kernel():
-    one = sq.hsum('g3_lbl', 1.0, 97, 1e-12, 1, split=0)
-    ls = sq.hsum('g3_lbl', 1.0, 97, 1e-12, 1, split=2)
-    assert ls['nev'] == one['nev'] and ls['nq'] == one['nq'] and ls['kept_top'] == one['kept_top']
-    assert abs(ls['S'][0] - one['S'][0]) <= 1e-11*abs(one['S'][0])
-    print('g3_lbl lockstep: S %.17g (single kernel %.17g)' % (ls['S'][0], one['S'][0]))
