@@ -48,6 +48,15 @@
                                  that spills its registers is built without it, keeping L1 for its stack */
 #endif
 #define SQB_QEPS 4.93e-32   /* double-double epsilon of the fallback's error model (driver/common.h:8) */
+#ifndef SQB_TABLE_GLOBAL
+#define SQB_TABLE_GLOBAL 0    /* FP64 pass: 1 = the lattice tables read through the read-only data cache instead of
+                                 from the CTA's shared-memory copy */
+#endif
+#if SQB_TABLE_GLOBAL
+#define SQB_TAB(p, j) __ldg((p) + (j))
+#else
+#define SQB_TAB(p, j) (p)[j]
+#endif
 
 /* The per-integral fields of a launch (sqb_inst_t) sit in shared memory: every thread of a CTA works on
  * one integral at a time.  A launch over one batch (ninst = 0) has one record, made from its own fields;
@@ -97,7 +106,7 @@ __device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const sqb_inst_t &
             int kd = p[d] - (((b >> d) & 1) ? st : 0);
             kk[d] = kd;
             if(kd < -K){ in = false; kd = -K; }
-            sf[d] = sX[kd + K]; ww = ww*sW[kd + K];
+            sf[d] = SQB_TAB(sX, kd + K); ww = ww*SQB_TAB(sW, kd + K);
         }
     } else {
         const short *p = (const short*)I.pts + c*(long)a.stride;
@@ -106,7 +115,7 @@ __device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const sqb_inst_t &
             int kd = p[d] - (((b >> d) & 1) ? st : 0);
             kk[d] = kd;
             if(kd < -K){ in = false; kd = -K; }
-            sf[d] = sX[kd + K]; ww = ww*sW[kd + K];
+            sf[d] = SQB_TAB(sX, kd + K); ww = ww*SQB_TAB(sW, kd + K);
         }
     }
     *w = ww;
@@ -242,7 +251,11 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
         int k = 0;
         if(multi){ if(t == 0) s_k = sqb_inst_at(a, tile*tl); __syncthreads(); k = s_k; }
         const sqb_inst_t &I = sI[k];
+#if SQB_TABLE_GLOBAL
+        const double *sX = I.X, *sW = I.Wt;
+#else
         const double *sX = sqb_sm + I.toff, *sW = sX + (2*I.K + 1);
+#endif
         const long base = multi ? tile*tl - I.child0 : tile*tl;     /* the tile's first point in its integral */
         const long n = multi ? (a.cells ? (I.n << D) : I.n) : n1;
         const long off = multi ? I.child0 : 0;                       /* global index = local index + off */
