@@ -226,8 +226,17 @@ static size_t table_bytes(const sqb_eval_t *a){
     return w*sizeof(double);
 }
 
+/* SQB_TILE_SUMS (environment, read once): 1 (default) = a level batch's FP64 kernel sums the tiles that
+ * need no fallback itself; 0 = the reduce kernel sums every tile */
+static int tile_sums(void){
+    static int v = -1;
+    if(v < 0){ const char *e = getenv("SQB_TILE_SUMS"); v = e && *e ? atoi(e) != 0 : 1; }
+    return v;
+}
+
 static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, long npts){
-    size_t smem = table_bytes(a);
+    /* the tables, then (level launches) the FP64 kernel's tile-sum columns */
+    size_t smem = table_bytes(a) + (a->part ? sizeof(sqb_tile_acc) : 0);
     sqb_dd_t d; memset(&d, 0, sizeof d);
     d.e = *a; d.dropunres = t->dropunres; d.uu = G.uu;
     if(t->alldd){
@@ -633,7 +642,9 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
          * pass: the reduce kernel sums every tile) */
         int can = 0;
         const long cap = grid_cap(g, f64_which(g, L->t.fma), 2*(2*G.K + 1)*sizeof(double), &can);
-        const bool fused = !L->t.alldd && can && !use_split(g, &a, &L->t) && nch >= 2*SQB_TILE*cap;
+        const bool fused = tile_sums() && !L->t.alldd && can && !use_split(g, &a, &L->t) && nch >= 2*SQB_TILE*cap;
+        /* the FP64 pass as a persistent grid taking tiles from the device queue (one integral: ninst = 1) */
+        const bool queue = !L->t.alldd && !use_split(g, &a, &L->t);
         /* the predictor at the last level: which children to leave out, and their tiers */
         if(pon){
             if(sqb_vtab_predict(L->vt, cells, nc, D, L->st, G.K, L->thr, L->predict, L->esok, L->sym, G.cfl,
@@ -642,6 +653,14 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
             a.cfl = G.cfl;
         }
         if(fused){ a.part = G.bp; a.tkeep = G.bkeep; a.tfb = G.tfb; a.pw = L->pw; a.thr = L->thr; a.last = L->last; }
+        if(queue){
+            a.part = G.bp; a.tkeep = G.bkeep; a.tfb = G.tfb;     /* every tile summed or flagged for the reduce */
+            a.ninst = 1; a.ntile = (nch + SQB_TILE - 1)/SQB_TILE; a.queue = G.queue;
+            sqb_inst_t &I = a.inst[0];
+            I.pts = cells; I.n = nc; I.child0 = 0; I.st = L->st; I.K = G.K; I.toff = 0; I.fused = fused;
+            I.last = L->last; I.pw = L->pw; I.thr = L->thr; I.abserr = L->t.abserr; I.near_thr = L->t.nearf*L->t.abserr;
+            I.X = G.X; I.Wt = G.Wt;
+        }
         if(eval_batch(g, &a, &L->t, nch)) return -1;
         lvl_t r; memset(&r, 0, sizeof r);
         r.cells = (const signed char*)cells; r.n = nch; r.D = D; r.st = L->st; r.last = L->last;
@@ -654,7 +673,7 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
             G.launches++;
         }
         const long nb = (nch + RTILE - 1)/RTILE;
-        sqb_k_reduce<<<(unsigned)nb, RT, 0, G.s>>>(r, G.bp, G.bkeep, fused ? G.tfb : NULL);
+        sqb_k_reduce<<<(unsigned)nb, RT, 0, G.s>>>(r, G.bp, G.bkeep, fused || queue ? G.tfb : NULL);
         CKR(cudaGetLastError());
         sqb_k_finish<<<1, FT, 0, G.s>>>(r, G.bp, G.bkeep, nb, G.boff, G.acc, G.base);
         CKR(cudaGetLastError());
@@ -759,7 +778,7 @@ extern "C" int sqb_dev_level_multi(const sqb_level_t *Ls, int n, sqb_acc_t *accs
             const long c0 = r*ncb[k], nc = L.ncell - c0 < ncb[k] ? L.ncell - c0 : ncb[k], nch = nc << D;
             sqb_inst_t &I = a.inst[m];
             I.pts = L.cells + c0; I.n = nc; I.child0 = child0; I.st = L.st; I.K = L.K; I.toff = toff;
-            I.fused = cank[k] && nch >= 2*SQB_TILE*capk[k];
+            I.fused = tile_sums() && cank[k] && nch >= 2*SQB_TILE*capk[k];
             I.last = L.last; I.pw = L.pw; I.thr = L.thr; I.abserr = L.t.abserr; I.near_thr = L.t.nearf*L.t.abserr;
             I.X = L.X; I.Wt = L.Wt;
             lvi_t &V = rl.inst[m];

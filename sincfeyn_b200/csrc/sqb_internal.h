@@ -32,6 +32,14 @@ typedef struct {
  * cell; the per-node flags byte (pt_t slot PFLAG) sits at element flag_at, or flag_at < 0. */
 /* the sums of one tile of SQB_TILE consecutive children of a level batch, double-double (hi, lo) */
 #define SQB_TILE 4096
+/* the FP64 kernel's running tile sums in level mode, one column per thread of its SQB_TILE_THREADS:
+ * dynamic shared memory after the launch's tables (the host adds its size to such launches) */
+#define SQB_TILE_THREADS 128
+typedef struct {
+    double S[2][SQB_TILE_THREADS], A[SQB_TILE_THREADS], dr[SQB_TILE_THREADS], b1[2][SQB_TILE_THREADS], b2[2][SQB_TILE_THREADS];
+    unsigned ne[SQB_TILE_THREADS], nsk[SQB_TILE_THREADS], keep[SQB_TILE_THREADS];
+    int fb;
+} sqb_tile_acc;
 typedef struct {
     double S[2], A[2], drop[2], b1[2], b2[2], u[2];
     unsigned long long ne, nq, unres, skipped;

@@ -178,11 +178,7 @@ __device__ __forceinline__ double sqb_point_test(const sqb_eval_t &a, const sqb_
 
 /* the tile's sums in level mode: thread t's running sums sit in shared memory (column t), out of the
  * registers that the integrand needs; at the tile's end warp 0 adds the columns in a fixed order */
-struct sqb_tile_acc {
-    double S[2][SQB_BLOCK], A[SQB_BLOCK], dr[SQB_BLOCK], b1[2][SQB_BLOCK], b2[2][SQB_BLOCK];
-    unsigned ne[SQB_BLOCK], nsk[SQB_BLOCK], keep[SQB_BLOCK];
-    int fb;
-};
+static_assert(SQB_BLOCK == SQB_TILE_THREADS, "the tile sums have one column per thread of the FP64 kernel's block");
 
 __device__ __forceinline__ void sqb_acc_dd(double (*x)[SQB_BLOCK], int t, double y){
     const sqdd z = sqdd_add_d(sqdd(x[0][t], x[1][t]), y);
@@ -234,7 +230,8 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
     __shared__ long s_tile;
     __shared__ int s_k;
 #if SQB_FUSE
-    __shared__ sqb_tile_acc ta;
+    /* the tile sums' columns follow the tables in dynamic shared memory (level launches only) */
+    sqb_tile_acc &ta = *(sqb_tile_acc*)(sqb_sm + sqb_table_words(a));
     const bool lvl = a.part != NULL;
 #else
     const bool lvl = false;

@@ -282,7 +282,7 @@ def all3():
         with open(ALL3_FILE, 'w') as f:
             json.dump(d, f, indent=1)
         print('%s %+.16e evals %d %.1f s' % (g, r['value'], r['evals'], r['time_s']), flush=True)
-    d['set_sum'] = sum(r['value']*r['w'] for r in d['rows'])
+    d['set_sum'] = sum(r['value'] for r in d['rows'])          # the value column includes the mirror weight
     d['reference_time_s'] = sum(r['time_s'] for r in d['rows'])
     with open(ALL3_FILE, 'w') as f:
         json.dump(d, f, indent=1)
