@@ -62,7 +62,7 @@ sys.path.insert(0, ROOT)
 H, N_PTS, EPS = 0.7, 139, 1e-12
 SET = 'all3'
 # the CPU sample: three-loop integrals of D = 5, 6, 6 and 7 at the workload's (h, N, eps); by points it is
-# mostly D = 7, as the set is (13 of its 41 integrals, about nine tenths of its points)
+# mostly D = 7, as the set is (12 of its 41 integrals, about nine tenths of its points)
 CPU_SAMPLE = ['g3_07', 'v3_01', 'g3_01', 'g3_00']
 # the precision sample: FP64 + dd against all-dd, two D = 7 graphs among them
 ALLDD_SAMPLE = ['v3_01', 'g3_07', 'g3_01', 'g3_00', 'g3_12']
@@ -205,7 +205,7 @@ def run_mixed(args, sq, L):
     rates = {}
     best, best_rate = None, -1.0
     for grp in (0, 1):
-        b, r = sq.batch_tune(sample, (1, 2, 4, 6, 8), group=grp)
+        b, r = sq.batch_tune(sample, (1, 2, 4, 8, 12, 16), group=grp)
         for w, v in r.items():
             rates['%s%d' % ('group_' if grp else '', w)] = v
             if v > best_rate:
@@ -663,7 +663,8 @@ def precision_table(args, sq, L, names, values, line):
             gold = {r['name']: r for r in json.load(f)['rows']}
         common = [g for g in names if g in gold and g in values]
         if common:
-            rel = {g: abs(values[g] - gold[g]['value'])/abs(gold[g]['value']) for g in common}
+            rel = {g: abs(values[g] - gold[g]['value'])/abs(gold[g]['value']) if gold[g]['value'] else abs(values[g])
+                   for g in common}
             worst = max(rel, key=rel.get)
             ref_sum = sum(gold[g]['value'] for g in common)
             out['vs_reference_cpu'] = {'integrals': len(common), 'max_rel': rel[worst], 'worst': worst,

@@ -79,6 +79,7 @@ typedef struct {
     int ninst;                    /* > 0: a multi-instance batch, the integrals in inst (the fields above that
                                      describe one batch unused); 0: one batch */
     lvi_t inst[SQB_MAXINST];
+    const unsigned char *cw;      /* list mode: every child's orbit weight from the select pass (0: not evaluated) */
 } lvl_t;
 
 struct Dev {
@@ -92,7 +93,8 @@ struct Dev {
     cudaEvent_t e0, e1;
     double *X, *Wt; int tabcap, K;
     long cap;                      /* points per batch */
-    double *v, *uu; unsigned char *stt, *cfl; long *fb; unsigned long long *nfb;
+    double *v, *uu; unsigned char *stt, *cfl, *cw; long *fb; unsigned long long *nfb;
+    unsigned long long *sel, *nsel;   /* list mode: the children to evaluate and their number */
     long nbcap; part_t *bp; unsigned *bkeep; unsigned long long *boff; unsigned char *tfb;
     long ttcap; double *tt, *ta;   /* split FP64 pass: running sums per point */
     sqb_acc_t *acc; unsigned long long *base;
@@ -150,6 +152,7 @@ extern "C" int sqb_dev_init(int device){
     CKR(cudaMalloc(&G.accm, SQB_MAXINST*sizeof(sqb_acc_t)));
     CKR(cudaMalloc(&G.basem, SQB_MAXINST*sizeof(unsigned long long)));
     CKR(cudaMalloc(&G.queue, sizeof(unsigned long long)));
+    CKR(cudaMalloc(&G.nsel, sizeof(unsigned long long)));
     G.on = 1;
     return 0;
 }
@@ -172,9 +175,11 @@ extern "C" int sqb_dev_tables(const double *X, const double *Wt, int K){
 static int reserve_points(long n){
     if(n <= G.cap) return 0;
     long c = 1L << 16; while(c < n) c <<= 1;
-    if(G.v){ cudaFree(G.v); cudaFree(G.uu); cudaFree(G.stt); cudaFree(G.cfl); cudaFree(G.fb); cudaFree(G.bp); cudaFree(G.bkeep); cudaFree(G.boff); cudaFree(G.tfb); }
+    if(G.v){ cudaFree(G.v); cudaFree(G.uu); cudaFree(G.stt); cudaFree(G.cfl); cudaFree(G.cw); cudaFree(G.fb); cudaFree(G.sel);
+             cudaFree(G.bp); cudaFree(G.bkeep); cudaFree(G.boff); cudaFree(G.tfb); }
     CKR(cudaMalloc(&G.v, c*sizeof(double))); CKR(cudaMalloc(&G.uu, c*sizeof(double)));
-    CKR(cudaMalloc(&G.stt, c)); CKR(cudaMalloc(&G.cfl, c)); CKR(cudaMalloc(&G.fb, c*sizeof(long)));
+    CKR(cudaMalloc(&G.stt, c)); CKR(cudaMalloc(&G.cfl, c)); CKR(cudaMalloc(&G.cw, c)); CKR(cudaMalloc(&G.fb, c*sizeof(long)));
+    CKR(cudaMalloc(&G.sel, c*sizeof(unsigned long long)));
     long nb = (c + RTILE - 1)/RTILE;
     CKR(cudaMalloc(&G.bp, nb*sizeof(part_t))); CKR(cudaMalloc(&G.bkeep, nb*sizeof(unsigned))); CKR(cudaMalloc(&G.tfb, nb));
     CKR(cudaMalloc(&G.boff, nb*sizeof(unsigned long long)));
@@ -412,6 +417,7 @@ __device__ __forceinline__ void child_of(const lvl_t &a, const lvi_t &L, long il
 }
 /* a present child's multiplicity: its orbit size under a fold, else 1 */
 __device__ __forceinline__ int child_weight(const lvl_t &a, const lvi_t &L, long il){
+    if(a.cw) return a.cw[il];
     if(a.sym.n <= 1) return 1;
     int k[SQB_MAXD];
     child_of(a, L, il, k);
@@ -603,6 +609,35 @@ __global__ void __launch_bounds__(RT) sqb_k_scatter(const __grid_constant__ lvl_
     }
 }
 
+/* list mode: the children of one level batch to evaluate -- in the box, not left out by the predictor and,
+ * under a fold, the minimum of their orbit (driver/sum.c:405-416) -- appended to sel as child index | orbit
+ * weight << SQB_SEL_SHIFT, in no particular order (each child's value and status go to its own slot, and
+ * the reduce kernel sums them in child order).  The other children get value 0 and no status; cw holds
+ * every child's weight (0: not evaluated) for the reduce and scatter kernels. */
+__global__ void __launch_bounds__(RT) sqb_k_select(const __grid_constant__ lvl_t a, int K, unsigned long long *sel,
+                                                   unsigned long long *nsel, double *v, unsigned char *stt,
+                                                   unsigned char *cw){
+    const lvi_t L = lvl_inst(a, 0);
+    const int lane = threadIdx.x & 31;
+    for(long b0 = blockIdx.x*(long)RT; b0 < a.n; b0 += (long)gridDim.x*RT){     /* the same trips for a warp */
+        const long i = b0 + threadIdx.x;
+        int mw = 0;
+        if(i < a.n){
+            int k[SQB_MAXD]; bool in = true;
+            child_of(a, L, i, k);
+            for(int d = 0; d < a.D; d++) in = in && k[d] >= -K;
+            if(in && !(a.cfl && (a.cfl[i] & 1))) mw = a.sym.n > 1 ? sqb_orbit_n(a.sym, k, a.D) : 1;
+            cw[i] = (unsigned char)mw;
+            if(!mw){ v[i] = 0; stt[i] = 0; }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, mw > 0);
+        unsigned long long base = 0;
+        if(lane == 0 && m) base = atomicAdd(nsel, (unsigned long long)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if(mw > 0) sel[base + __popc(m & ((1u << lane) - 1))] = (unsigned long long)i | ((unsigned long long)mw << SQB_SEL_SHIFT);
+    }
+}
+
 extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n, double *ms){
     const sqb_graph_t *g = L->g; const int D = g->D;
     long maxch = L->max_children > 0 ? L->max_children : (1L << 25);
@@ -642,9 +677,12 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
          * pass: the reduce kernel sums every tile) */
         int can = 0;
         const long cap = grid_cap(g, f64_which(g, L->t.fma), 2*(2*G.K + 1)*sizeof(double), &can);
-        const bool fused = tile_sums() && !L->t.alldd && can && !use_split(g, &a, &L->t) && nch >= 2*SQB_TILE*cap;
-        /* the FP64 pass as a persistent grid taking tiles from the device queue (one integral: ninst = 1) */
+        /* the FP64 pass as a persistent grid taking tiles from the device queue (one integral: ninst = 1);
+         * under a fold or the predictor it walks the list of children to evaluate (list mode), and the
+         * reduce kernel sums every tile */
         const bool queue = !L->t.alldd && !use_split(g, &a, &L->t);
+        const bool listm = queue && (a.sym.n > 1 || pon);
+        const bool fused = tile_sums() && !L->t.alldd && can && !use_split(g, &a, &L->t) && !listm && nch >= 2*SQB_TILE*cap;
         /* the predictor at the last level: which children to leave out, and their tiers */
         if(pon){
             if(sqb_vtab_predict(L->vt, cells, nc, D, L->st, G.K, L->thr, L->predict, L->esok, L->sym, G.cfl,
@@ -661,18 +699,28 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
             I.last = L->last; I.pw = L->pw; I.thr = L->thr; I.abserr = L->t.abserr; I.near_thr = L->t.nearf*L->t.abserr;
             I.X = G.X; I.Wt = G.Wt;
         }
-        if(eval_batch(g, &a, &L->t, nch)) return -1;
         lvl_t r; memset(&r, 0, sizeof r);
         r.cells = (const signed char*)cells; r.n = nch; r.D = D; r.st = L->st; r.last = L->last;
         r.abskip = L->t.abskip; r.pw = L->pw; r.thr = L->thr; r.v = G.v; r.uu = G.uu; r.stt = G.stt;
         r.sym = a.sym; r.cfl = a.cfl;
+        const long nb = (nch + RTILE - 1)/RTILE;
+        if(listm){
+            CKR(cudaMemsetAsync(G.nsel, 0, sizeof(unsigned long long), G.s));
+            CKR(cudaMemsetAsync(G.tfb, 1, nb, G.s));
+            const long want = (nch + RT - 1)/RT, full = (long)G.nsm*8;
+            sqb_k_select<<<(unsigned)(want < full ? want : full), RT, 0, G.s>>>(r, G.K, G.sel, G.nsel, G.v, G.stt, G.cw);
+            CKR(cudaGetLastError());
+            G.launches++;
+            a.sel = G.sel; a.nsel = G.nsel;
+            r.cw = G.cw;
+        }
+        if(eval_batch(g, &a, &L->t, nch)) return -1;
         /* the level before the last stores its values for the predictor */
         if(L->vput && L->vt){
             if(sqb_vtab_put_children(L->vt, cells, nch, D, L->st, G.v, G.stt, L->sym, G.s)){
                 snprintf(g_err, sizeof g_err, "%s", sqb_vtab_error()); return -1; }
             G.launches++;
         }
-        const long nb = (nch + RTILE - 1)/RTILE;
         sqb_k_reduce<<<(unsigned)nb, RT, 0, G.s>>>(r, G.bp, G.bkeep, fused || queue ? G.tfb : NULL);
         CKR(cudaGetLastError());
         sqb_k_finish<<<1, FT, 0, G.s>>>(r, G.bp, G.bkeep, nb, G.boff, G.acc, G.base);

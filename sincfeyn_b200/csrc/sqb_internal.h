@@ -99,7 +99,13 @@ typedef struct {
     long ntile;
     unsigned long long *queue;
     sqb_inst_t inst[SQB_MAXINST];
+    /* list mode (one integral's level batch under a fold or the predictor): the children to evaluate, as
+     * child index | orbit weight << 56, *nsel of them, written by the select pass, which also zeroed the
+     * others; the FP64 kernel walks the list (tiles of SQB_TILE entries from the queue) and leaves every
+     * tile's sums to the reduce kernel */
+    const unsigned long long *sel, *nsel;
 } sqb_eval_t;
+#define SQB_SEL_SHIFT 56
 
 /* The double-double kernel over a list of points of the same launch geometry (fb/nfb from the FP64
  * pass), or over every point (all = 1: the all-double-double form). */

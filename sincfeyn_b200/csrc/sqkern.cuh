@@ -84,7 +84,7 @@ __host__ __device__ __forceinline__ int sqb_table_words(const sqb_eval_t &a){
  * returns 0 for a child below the box, a child the predictor leaves out or, under a symmetry fold, a child
  * that is not the minimum of its orbit (driver/sum.c:405-416), else the point's multiplicity (the orbit
  * size; 1 without a fold) */
-template<int D>
+template<int D, bool ORB = true>
 __device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const sqb_inst_t &I, const double *sX, const double *sW,
                                          long il, long ig, long *cell, double *sf, double *w){
     long c; int b;
@@ -121,6 +121,7 @@ __device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const sqb_inst_t &
     *w = ww;
     if(!in) return 0;
     if(a.cfl && (a.cfl[ig] & 1)) return 0;          /* left out by the predictor */
+    if constexpr(!ORB) return 1;               /* list mode: the select pass has the orbit weight */
     return a.cells && a.sym.n > 1 ? sqb_orbit<D>(a.sym, kk) : 1;
 }
 
@@ -178,7 +179,9 @@ __device__ __forceinline__ double sqb_point_test(const sqb_eval_t &a, const sqb_
 
 /* the tile's sums in level mode: thread t's running sums sit in shared memory (column t), out of the
  * registers that the integrand needs; at the tile's end warp 0 adds the columns in a fixed order */
+#if SQB_FUSE
 static_assert(SQB_BLOCK == SQB_TILE_THREADS, "the tile sums have one column per thread of the FP64 kernel's block");
+#endif
 
 __device__ __forceinline__ void sqb_acc_dd(double (*x)[SQB_BLOCK], int t, double y){
     const sqdd z = sqdd_add_d(sqdd(x[0][t], x[1][t]), y);
@@ -240,7 +243,8 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
     const bool multi = a.ninst > 0;
     const long n1 = multi ? 0 : (a.cells ? (a.n << D) : a.n);      /* one batch: its points */
     const long tl = (lvl || multi) ? SQB_TILE : SQB_BLOCK;          /* other modes: one point per thread per step */
-    const long ntiles = multi ? a.ntile : (n1 + tl - 1)/tl;
+    const long nsel = a.sel ? (long)*a.nsel : 0;                    /* list mode (one integral, queue): its entries */
+    const long ntiles = a.sel ? (nsel + tl - 1)/tl : multi ? a.ntile : (n1 + tl - 1)/tl;
     const int t = threadIdx.x;
     long tile = blockIdx.x;
     if(multi){ if(t == 0) s_tile = (long)atomicAdd(a.queue, 1ULL); __syncthreads(); tile = s_tile; }
@@ -257,7 +261,7 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
         const long n = multi ? (a.cells ? (I.n << D) : I.n) : n1;
         const long off = multi ? I.child0 : 0;                       /* global index = local index + off */
 #if SQB_FUSE
-        const bool tsum = lvl && I.fused;
+        const bool tsum = lvl && I.fused && !a.sel;
         if(tsum){
             ta.S[0][t] = ta.S[1][t] = ta.A[t] = ta.dr[t] = ta.b1[0][t] = ta.b1[1][t] = ta.b2[0][t] = ta.b2[1][t] = 0;
             ta.ne[t] = ta.nsk[t] = ta.keep[t] = 0;
@@ -268,10 +272,20 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
         const bool tsum = false;
 #endif
         for(int j = 0; j < tl/SQB_BLOCK; j++){
-            const long il = base + (long)j*SQB_BLOCK + t, i = il + off;
-            if(il >= n) break;
+            long il, i; int mw;
             long c; double sf[D], w;
-            const int mw = sqb_point<D>(a, I, sX, sW, il, i, &c, sf, &w);
+            if(a.sel){
+                const long q = tile*tl + (long)j*SQB_BLOCK + t;
+                if(q >= nsel) break;
+                const unsigned long long e = a.sel[q];
+                il = i = (long)(e & ((1ULL << SQB_SEL_SHIFT) - 1));
+                sqb_point<D, false>(a, I, sX, sW, il, i, &c, sf, &w);
+                mw = (int)(e >> SQB_SEL_SHIFT);
+            } else {
+                il = base + (long)j*SQB_BLOCK + t; i = il + off;
+                if(il >= n) break;
+                mw = sqb_point<D>(a, I, sX, sW, il, i, &c, sf, &w);
+            }
             if(!mw){
                 a.v[i] = 0;
                 if(a.raw) a.ab[i] = 0; else a.stt[i] = 0;
@@ -312,7 +326,7 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
             __syncthreads();
         } else
 #endif
-        if(multi && a.tfb && t == 0) a.tfb[tile] = 1;                /* summed by the reduce kernel */
+        if(multi && a.tfb && !a.sel && t == 0) a.tfb[tile] = 1;      /* summed by the reduce kernel */
         if(multi){
             __syncthreads();                                          /* every thread has read s_tile, s_k */
             if(t == 0) s_tile = (long)atomicAdd(a.queue, 1ULL);
