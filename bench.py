@@ -261,7 +261,7 @@ def run_vp4(args, sq, L):
     at h = 1.0 (N = 97) and 0.9 (N = 107), eps = 1e-12, as one concurrent batch per h; the device time,
     points/s, and each lepton-loop set's sum against its exact value."""
     import torch
-    names = sq.select(['vp4'])
+    names = [n for n in sq.select(['vp4']) if not n.startswith('w4_p6')]     # kernels/v4 and kernels/w4 (not pi6)
     info = {g['name']: g for g in sq.graphs()}
     for g in names:
         sq.preload(g)

@@ -33,7 +33,7 @@ LIB = os.path.join(PKG, 'lib')
 BIN = os.path.join(PKG, 'bin')
 INC = os.path.join(ROOT, 'include')
 DEFAULT_KERNELS = os.environ.get('SQB_KERNELS')     # the reference's kernels/ directory (no default)
-DEFAULT_CLASSES = os.environ.get('SQB_CLASSES', 'g2 g3 v3 v4 w4')
+DEFAULT_CLASSES = os.environ.get('SQB_CLASSES', 'g2 g3 v3 v4 w4 pi6')
 
 NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']

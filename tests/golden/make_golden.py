@@ -222,12 +222,14 @@ def mixed2():
 VP4_H = ((1.0, 97), (0.9, 107))
 # a dimension-stratified sample of kernels/v4 and kernels/w4 (D = 6, 7, 8, 9; the cheapest D = 9 graph at
 # h = 2.0), and the lepton-loop sets I(a), I(b), I(c) of docs/LEPTON_LOOPS.md:5-17
-VP4_SAMPLE = ['w4_00Sc', 'v4_00', 'w4_00Sm', 'w4_00Vm', 'w4_0iSc', 'w4_0iSm', 'w4_0iVm', 'v4_02', 'v4_14']
+VP4_SAMPLE = {1.0: ['w4_00Sc', 'v4_00', 'w4_00Sm', 'w4_00Vm', 'w4_0iSc', 'w4_0iSm', 'w4_0iVm', 'v4_02', 'v4_14'],
+              0.9: ['w4_00Sc', 'v4_00', 'w4_00Sm', 'w4_0iSc', 'w4_0iSm', 'v4_02']}     # D = 6..8 at h = 0.9
 VP4_FILE = os.path.join(OUT, 'vp4_sample.json')
 
 
 def vp4():
-    """`sincqed run h N 1e-12 GRAPH` for VP4_SAMPLE at h = 1.0 (N = 97) and 0.9 (N = 107), default top = 1:
+    """`sincqed run h N 1e-12 GRAPH` for VP4_SAMPLE at h = 1.0 (N = 97; D = 6..9) and 0.9 (N = 107; D = 6..8, the
+    D = 9 graph alone being hours of CPU time there), default top = 1:
     the -ffp-contract=off build, SINCQED_SYM=0, SINCQED_KEEPBT=1, one graph per process (checkpoints every
     15 min; the file is rewritten after every run and runs already in it are kept)"""
     d = {'env': {'SINCQED_SYM': '0', 'SINCQED_KEEPBT': '1'}, 'eps': 1e-12, 'threads': os.cpu_count(),
@@ -239,7 +241,7 @@ def vp4():
     ck = os.path.join(tempfile.gettempdir(), 'sincfeyn_golden_ckpt')
     os.makedirs(ck, exist_ok=True)
     for h, N in VP4_H:
-        for g in VP4_SAMPLE:
+        for g in VP4_SAMPLE[h]:
             if (g, h) in done:
                 continue
             env = dict(d['env'], SINCQED_CKPT='900', SINCQED_CKPT_DIR=ck)

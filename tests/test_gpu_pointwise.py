@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 NOT_BITWISE = {'g3_lbl'}
 
 
-@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3', 'v4', 'w4'])
+@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3', 'v4', 'w4', 'pi6'])
 def test_fp64_and_dd_bitwise(cls):
     z = np.load(os.path.join(GOLD, 'pointwise_%s.npz' % cls))
     have = {g['name'] for g in sq.graphs()}
@@ -44,7 +44,7 @@ def test_fp64_and_dd_bitwise(cls):
     assert not bad, bad
 
 
-@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3', 'v4', 'w4'])
+@pytest.mark.parametrize('cls', ['g2', 'v3', 'g3', 'v4', 'w4', 'pi6'])
 def test_contracted_fp64_within_rounding(cls):
     """The contracted FP64 kernels (fused multiply-adds, the default fast form) round differently from
     the source; at the same nodes they agree with the reference double half to a few ulp of the |.| sum,
