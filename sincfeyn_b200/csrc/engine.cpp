@@ -166,9 +166,10 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
         v.resize(n); stt.resize(n); cls.resize(n);
         const double *vd; const unsigned char *sd;
         const double t0 = now();
+        if(sqb_grow_shells_async()) FAIL("device grow: %s", sqb_top_error());
         if(sqb_dev_eval_resident(R.g, pts, n, skip, &R.t, v.data(), stt.data(), &R.nq, &R.u, &R.unresdrop, &vd, &sd))
             FAIL("device: %s", sqb_last_error());
-        if(sqb_grow_shells(cls.data())) FAIL("device grow: %s", sqb_top_error());
+        sqb_grow_shells_take(cls.data());
         /* the predictor stores every grow value (driver/sumkey.h:219-222) */
         if(R.vt && (sqb_vtab_reserve(R.vt, n, sqb_dev_stream()) || sqb_vtab_put_nodes(R.vt, pts, vd, n, R.D, sqb_dev_stream())))
             FAIL("predictor: %s", sqb_vtab_error());

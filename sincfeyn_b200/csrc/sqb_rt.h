@@ -102,7 +102,8 @@ void *sqb_dev_stream(void);
 /* the top level on the device (topgrid.cu): grow frontiers, final threshold, tiers, dilation */
 int  sqb_grow_begin(int D, int K, int st, int W, const unsigned long long *P, int gs, int abskip, void *stream);
 long sqb_grow_frontier(const sqb_pt_t **pts, const unsigned char **skip);
-int  sqb_grow_shells(unsigned char *cls_host);
+int  sqb_grow_shells_async(void);
+void sqb_grow_shells_take(unsigned char *cls_host);
 int  sqb_grow_expand(const double *v_dev, const unsigned char *stt_dev, double thr, long *nkept, long *nnext);
 int  sqb_grow_kv(double *kv_host, long n);
 int  sqb_grow_finish(double thr, int tiers, long *m);

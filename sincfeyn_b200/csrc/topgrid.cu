@@ -162,6 +162,8 @@ struct Grow {
     long *qs; long qscap;                                                        /* slot per candidate */
     unsigned long long *err;
     int gs, abskip;
+    unsigned char *hcls; long hclscap;     /* pinned: the frontier's shell classes, read after the next sync */
+    unsigned long long *herr;              /* pinned: the overflow count, read after the next sync */
 };
 static thread_local Grow GR;
 
@@ -257,14 +259,24 @@ __global__ void k_shell(const sqb_pt_t *fr, long n, geom_t g, unsigned char *cls
         cls[i] = mx == g.K ? 2 : (mx == g.K - g.st ? 4 : 0);
     }
 }
-extern "C" int sqb_grow_shells(unsigned char *cls_host){
+/* the frontier's shell classes: the kernel and the copy to pinned memory are queued on the grow's stream
+ * without waiting (sqb_grow_shells_async, before the frontier's evaluation, whose results the caller waits
+ * for anyway), and sqb_grow_shells_take copies them out after that wait */
+extern "C" int sqb_grow_shells_async(void){
     if(!GR.nfr) return 0;
+    if(GR.nfr > GR.hclscap){
+        if(GR.hcls) cudaFreeHost(GR.hcls);
+        long c = 1L << 16; while(c < GR.nfr) c <<= 1;
+        TCK(cudaMallocHost(&GR.hcls, c)); GR.hclscap = c;
+    }
     k_shell<<<1184, 256, 0, TS>>>(GR.fr, GR.nfr, GR.g, GR.cls); TL++;
     TCK(cudaGetLastError());
-    TCK(cudaMemcpyAsync(cls_host, GR.cls, GR.nfr, cudaMemcpyDeviceToHost, TS));
-    TCK(cudaStreamSynchronize(TS));
+    TCK(cudaMemcpyAsync(GR.hcls, GR.cls, GR.nfr, cudaMemcpyDeviceToHost, TS));
     sqb_dev_count_copy(0, GR.nfr);
     return 0;
+}
+extern "C" void sqb_grow_shells_take(unsigned char *cls_host){
+    if(GR.nfr) memcpy(cls_host, GR.hcls, GR.nfr);
 }
 
 struct KeepOp {                  /* kept frontier points appended to the keep list, their index to kj */
@@ -332,6 +344,9 @@ extern "C" int sqb_grow_expand(const double *v_dev, const unsigned char *stt_dev
     if(frontier_room(nc)) return -1;
     if(nc){ k_claim<<<1184, 256, 0, TS>>>(GR.g, GR.fr, GR.kj, nk, GR.key, GR.word, GR.mask, GR.qs, GR.err); TL++; }
     TCK(cudaGetLastError());
+    /* the overflow count after the claims (the only writers), read once the next compaction has waited */
+    if(!GR.herr) TCK(cudaMallocHost(&GR.herr, sizeof(unsigned long long)));
+    TCK(cudaMemcpyAsync(GR.herr, GR.err, sizeof(unsigned long long), cudaMemcpyDeviceToHost, TS));
     WinOp wo; wo.fr = GR.fr; wo.kj = GR.kj; wo.qs = GR.qs; wo.word = GR.word; wo.frsk = GR.frsk; wo.stt = stt_dev;
     wo.nx = GR.nx; wo.nxsk = GR.nxsk; wo.D2 = 2*GR.g.D; wo.st = GR.g.st; wo.gs = GR.gs;
     long nn = 0;
@@ -339,10 +354,8 @@ extern "C" int sqb_grow_expand(const double *v_dev, const unsigned char *stt_dev
     GR.nseen += nn;
     { sqb_pt_t *t = GR.fr; GR.fr = GR.nx; GR.nx = t; unsigned char *q = GR.frsk; GR.frsk = GR.nxsk; GR.nxsk = q; }
     GR.nfr = nn; *nnext = nn;
-    unsigned long long e = 0;
-    TCK(cudaMemcpyAsync(&e, GR.err, sizeof e, cudaMemcpyDeviceToHost, TS));
-    TCK(cudaStreamSynchronize(TS));
-    if(e){ snprintf(terr, sizeof terr, "grow: hash table overflow"); return -1; }
+    if(nc <= 0) TCK(cudaStreamSynchronize(TS));          /* no compaction waited for the copy */
+    if(*GR.herr){ snprintf(terr, sizeof terr, "grow: hash table overflow"); return -1; }
     return 0;
 }
 
