@@ -209,14 +209,6 @@ static int grid_for(const sqb_graph_t *g, int which, long npts, size_t smem){
     if(want < 1) want = 1;
     return (int)(want < full ? want : full);
 }
-/* an FP64 launch over npts nodes or children outside the level batches (the plug-in, pointwise checks,
- * grow frontiers): one CTA per 128 points, which the hardware schedules as others finish (measured faster
- * than a resident-size grid that walks the points in turn) */
-static int grid_points(long npts){
-    long want = (npts + 127)/128;
-    if(want < 1) want = 1;
-    return (int)(want < 0x7FFFFFFFL ? want : 0x7FFFFFFFL);
-}
 
 static void fill_eval(sqb_eval_t *a, const sqb_test_t *t){
     a->X = G.X; a->Wt = G.Wt; a->K = G.K; a->H = 0; a->raw = 0;
@@ -283,7 +275,7 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
             CKR(cudaMemsetAsync(a->queue, 0, sizeof(unsigned long long), G.s));
             const long cap = grid_cap(g, w, smem);
             launch_f64(g, w, a, (int)(a->ntile < cap ? a->ntile : cap), smem, G.s);
-        } else launch_f64(g, w, a, grid_points(npts), smem, G.s);
+        } else launch_f64(g, w, a, grid_for(g, w, npts, smem), smem, G.s);
         CKR(cudaGetLastError());
     }
     if(ev) CKR(cudaEventRecord(ev[1], G.s));
@@ -960,7 +952,7 @@ static void plain_launch(pslot_t *s, long npts, long nrows, int cells, int st, i
     a.X = PEX; a.Wt = NULL; a.K = PK; a.H = PH; a.raw = 1; a.skip = has_skip ? s->dS : NULL;
     a.v = s->dF; a.ab = s->dA;
     size_t smem = 2*(2*PK + 1)*sizeof(double);
-    PCUR->f64(&a, grid_points(npts), 128, smem, s->st);
+    PCUR->f64(&a, grid_for(PCUR, 0, npts, smem), 128, smem, s->st);
     CKX(cudaGetLastError());
 }
 
@@ -1008,7 +1000,7 @@ extern "C" void sqb_gg_launch(const sqb_graph_t *g, void *st, long n, const shor
     a.pts = k; a.n = cmode ? (n >> g->D) : n; a.esize = 2; a.stride = g->D; a.flag_at = -1; a.cells = cmode; a.st = cst;
     a.X = EX; a.Wt = NULL; a.K = K; a.H = H; a.raw = 1; a.skip = skip; a.v = of; a.ab = oab;
     size_t smem = 2*(2*K + 1)*sizeof(double);
-    g->f64(&a, grid_points(n), 128, smem, st);
+    g->f64(&a, grid_for(g, 0, n, smem), 128, smem, st);
 }
 
 /* GG_<graph>'s launcher with the FP64 build chosen (0 as written, 2 contracted) */
@@ -1026,7 +1018,7 @@ extern "C" int sqb_plugin_launch(const char *graph, int form, cudaStream_t st, l
     a.pts = k; a.n = cmode ? (n >> g->D) : n; a.esize = 2; a.stride = g->D; a.flag_at = -1; a.cells = cmode; a.st = cst;
     a.X = EX; a.Wt = NULL; a.K = K; a.H = H; a.raw = 1; a.skip = skip; a.v = of; a.ab = oab;
     const size_t smem = 2*(2*K + 1)*sizeof(double);
-    launch_f64(g, form, &a, grid_points(n), smem, st);
+    launch_f64(g, form, &a, grid_for(g, form, n, smem), smem, st);
     const cudaError_t e = cudaGetLastError();
     if(e != cudaSuccess){
         snprintf(g_err, sizeof g_err, "sqb_plugin_launch: %s", cudaGetErrorString(e)); sqb_set_error_msg(g_err); return (int)e; }
@@ -1058,7 +1050,7 @@ extern "C" int sqb_eval_points_impl(const sqb_graph_t *g, long n, const double *
     if(prec == 0 || prec == 2){
         const int w = f64_which(g, prec == 2);
         if(prec == 2 && w != 2){ snprintf(g_err, sizeof g_err, "%s: no contracted FP64 kernel in this library", g->name); rc = -1; }
-        else launch_f64(g, w, &a, grid_points(n), smem, G.s);
+        else launch_f64(g, w, &a, grid_for(g, w, n, smem), smem, G.s);
     } else { sqb_dd_t d; memset(&d, 0, sizeof d); d.e = a; d.all = 1; d.uu = dvl; g->dd(&d, grid_for(g, 1, n, smem), 128, smem, G.s); }
     if(!rc){
         CKR(cudaGetLastError());
