@@ -65,7 +65,7 @@ def _flags_stamp():
     input of every such unit, rewritten -- so newer than the objects -- only when the policy changes.  A
     first stamp is dated to the epoch: objects already built are taken to follow the policy."""
     path = os.path.join(BUILD, 'fma_policy.txt')
-    text = json.dumps({'flags': NVFLAGS_FMA, 'spill_max': SPILL_MAX}) + '\n'
+    text = json.dumps({'flags': NVFLAGS_FMA, 'spill_max': SPILL_MAX, 'sweeps_flops': SWEEPS_FLOPS}) + '\n'
     old = open(path).read() if os.path.exists(path) else None
     if old != text:
         os.makedirs(BUILD, exist_ok=True)
@@ -92,26 +92,42 @@ OCC = os.path.join(LIB, 'occupancy.json')
 # kernels of the D = 7 three-loop graphs run 7-9 % faster, while g3_lbl, which would spill kilobytes,
 # runs slower capped.
 SPILL_MAX = 128
-_PTXAS_F64 = re.compile(r'Function properties for _Z9sqb_k_f64\S*\s*\n\s*(\d+) bytes stack frame, (\d+) bytes spill stores')
+# The contracted unit's level kernel takes a batch's tiles in two sweeps (SQB_SWEEPS = 2: the children of
+# cells that skip the |.| sums, then the others) for integrands of at least SWEEPS_FLOPS algorithmic flops
+# per point with cells of at least 32 children: measured on the B200 at 50 % skipped cells, the two forms of
+# such a point function interleaved on one SM run 1.3-1.6x slower than either alone (v4_65, 5,520 flops;
+# w4_07Vm, 9,313; g3_lbl, 25,307), while g3_00's (2,137) do not.
+SWEEPS_FLOPS = 4000
+# the point function's spill stores: the contracted unit calls it (sqb_fcall, one copy per kernel); the
+# exact unit inlines it into sqb_k_f64
+_PTXAS_SPILL = re.compile(r'Function properties for (_Z9sqb_fcall|_Z9sqb_k_f64)\S*\s*\n\s*(\d+) bytes stack frame, (\d+) bytes spill stores')
 
 
-def _compile_graph(tu, o, tuf, of, name, do_exact, do_fma):
-    """Both units of one graph.  A graph whose contracted kernel spills even at the uncapped allocation
-    (g3_lbl: ~1 KB of stack per thread) is built without the level-mode tile sums in both units: their
-    shared memory would take L1 from the stack it spills to (measured: g3_lbl 15 % slower with them)."""
+def _spill(out):
+    """The largest spill-store count ptxas reports for the point function (its calls if there are any,
+    else the FP64 kernels); -1 if it reports none."""
+    found = [(m.group(1), int(m.group(3))) for m in _PTXAS_SPILL.finditer(out)]
+    calls = [v for k, v in found if k == '_Z9sqb_fcall']
+    vals = calls or [v for k, v in found]
+    return max(vals) if vals else -1
+
+
+def _compile_graph(tu, o, tuf, of, name, do_exact, do_fma, sweeps=1):
+    """Both units of one graph.  A graph whose contracted point function spills even at the uncapped
+    allocation (g3_lbl: ~1 KB of stack per thread) is built without the level-mode tile sums in both units:
+    their shared memory would take L1 from the stack it spills to (measured: g3_lbl 15 % slower with them)."""
     info = None
     if do_fma:
-        out = _run([NVCC] + NVFLAGS_FMA + ['-DSQB_MINB=3', '-Xptxas', '-v', '-I' + GEN, '-c', tuf, '-o', of])
-        m = _PTXAS_F64.search(out)
-        spill = int(m.group(2)) if m else -1
-        info = {'min_blocks': 3, 'spill_stores_at_3': spill, 'fused': 1}
+        sw = ['-DSQB_SWEEPS=2'] if sweeps > 1 else []
+        out = _run([NVCC] + NVFLAGS_FMA + sw + ['-DSQB_MINB=3', '-Xptxas', '-v', '-I' + GEN, '-c', tuf, '-o', of])
+        spill = _spill(out)
+        info = {'min_blocks': 3, 'spill_stores_at_3': spill, 'fused': 1, 'sweeps': sweeps}
         if spill < 0 or spill > SPILL_MAX:
-            out = _run([NVCC] + NVFLAGS_FMA + ['-Xptxas', '-v', '-I' + GEN, '-c', tuf, '-o', of])
-            m = _PTXAS_F64.search(out)
-            spill1 = int(m.group(2)) if m else -1
-            info = {'min_blocks': 1, 'spill_stores_at_3': spill, 'spill_stores_at_1': spill1, 'fused': 1}
+            out = _run([NVCC] + NVFLAGS_FMA + sw + ['-Xptxas', '-v', '-I' + GEN, '-c', tuf, '-o', of])
+            spill1 = _spill(out)
+            info = {'min_blocks': 1, 'spill_stores_at_3': spill, 'spill_stores_at_1': spill1, 'fused': 1, 'sweeps': sweeps}
             if spill1 < 0 or spill1 > SPILL_MAX:
-                _run([NVCC] + NVFLAGS_FMA + ['-DSQB_FUSE=0', '-I' + GEN, '-c', tuf, '-o', of])
+                _run([NVCC] + NVFLAGS_FMA + sw + ['-DSQB_FUSE=0', '-I' + GEN, '-c', tuf, '-o', of])
                 info['fused'] = 0
     elif os.path.exists(OCC):
         with open(OCC) as f:
@@ -273,7 +289,8 @@ def build(kernels=DEFAULT_KERNELS, classes=DEFAULT_CLASSES, jobs=None, verbose=T
         do_fma = _newer(of, [tuf, cuh, stamp] + khdrs)
         do_exact = do_fma or _newer(o, [tu, cuh] + khdrs)
         if do_fma or do_exact:
-            jobs_list.append(lambda a=(tu, o, tuf, of, name, do_exact, do_fma): _compile_graph(*a))
+            sweeps = 2 if D >= 5 and flops.get(name, {}).get('ab1', 0) >= SWEEPS_FLOPS else 1
+            jobs_list.append(lambda a=(tu, o, tuf, of, name, do_exact, do_fma, sweeps): _compile_graph(*a))
     rt_o = os.path.join(OBJ, 'runtime.o')
     if _newer(rt_o, [os.path.join(CSRC, 'runtime.cu')] + hdrs):
         jobs_list.append([NVCC] + NVFLAGS + ['-Xcompiler', '-fopenmp', '-c', os.path.join(CSRC, 'runtime.cu'), '-o', rt_o])

@@ -193,12 +193,14 @@ static inline void launch_f64(const sqb_graph_t *g, int which, const sqb_eval_t 
     if(which == 2) g->f64_fma(a, grid, 128, smem, s); else g->f64(a, grid, 128, smem, s);
 }
 
-/* resident CTAs of a graph's kernel on the whole device; *fused: the kernel sums level tiles itself */
-static long grid_cap(const sqb_graph_t *g, int which, size_t smem, int *fused = NULL){
+/* resident CTAs of a graph's kernel on the whole device (which | SQB_ATTR_LEVEL: its level kernel); *fused:
+ * the kernel sums level tiles itself; *sweeps: the level kernel's passes over a batch's tiles */
+static long grid_cap(const sqb_graph_t *g, int which, size_t smem, int *fused = NULL, int *sweeps = NULL){
     sqb_kattr_t at; memset(&at, 0, sizeof at); int per = 2;
     const int ok = g->attr(which, 128, smem, &at);
     if(ok && at.blocks_per_sm > 0) per = at.blocks_per_sm;
     if(fused) *fused = ok && at.fused;
+    if(sweeps) *sweeps = ok && at.sweeps > 1 ? at.sweeps : 1;
     return (long)G.nsm*per;
 }
 
@@ -273,8 +275,10 @@ static int eval_batch(const sqb_graph_t *g, sqb_eval_t *a, const sqb_test_t *t, 
         const int w = f64_which(g, t->fma);
         if(a->ninst > 0){
             CKR(cudaMemsetAsync(a->queue, 0, sizeof(unsigned long long), G.s));
-            const long cap = grid_cap(g, w, smem);
-            launch_f64(g, w, a, (int)(a->ntile < cap ? a->ntile : cap), smem, G.s);
+            int sw = 1;
+            const long cap = grid_cap(g, w | (sqb_level_launch(a) ? SQB_ATTR_LEVEL : 0), smem, NULL, &sw);
+            const long items = a->ntile*sw;       /* the level kernel may take every tile twice */
+            launch_f64(g, w, a, (int)(items < cap ? items : cap), smem, G.s);
         } else launch_f64(g, w, a, grid_for(g, w, npts, smem), smem, G.s);
         CKR(cudaGetLastError());
     }
@@ -648,7 +652,7 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
      * finish one more */
     {
         int can0 = 0;
-        const long cap0 = grid_cap(g, f64_which(g, L->t.fma), 2*(2*G.K + 1)*sizeof(double), &can0);
+        const long cap0 = grid_cap(g, f64_which(g, L->t.fma) | SQB_ATTR_LEVEL, 2*(2*G.K + 1)*sizeof(double), &can0);
         const long round = (cap0*SQB_TILE) >> D;            /* cells per round (SQB_TILE >= 2^D) */
         if(!L->t.alldd && can0 && round > 0 && ncb >= 2*round) ncb = (ncb/round)*round;
     }
@@ -675,8 +679,6 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
         }
         /* level mode: the FP64 pass sums the tiles without fallback points (the all-dd form has no FP64
          * pass: the reduce kernel sums every tile) */
-        int can = 0;
-        const long cap = grid_cap(g, f64_which(g, L->t.fma), 2*(2*G.K + 1)*sizeof(double), &can);
         /* the FP64 pass as a persistent grid taking tiles from the device queue (one integral: ninst = 1);
          * under a fold or the predictor it walks the list of children to evaluate (list mode), and the
          * reduce kernel sums every tile */
@@ -685,6 +687,10 @@ extern "C" int sqb_dev_level(const sqb_level_t *L, sqb_acc_t *acc, long *next_n,
          * 4 or more, or the predictor (measured on four-loop VP integrals: order 8, 1.5x faster; order 2,
          * 16 % slower than testing in place) */
         const bool listm = queue && (a.sym.n >= 4 || pon);
+        /* the kernel that runs: the level kernel for a queue batch outside list mode */
+        int can = 0;
+        const long cap = grid_cap(g, f64_which(g, L->t.fma) | (queue && !listm ? SQB_ATTR_LEVEL : 0),
+                                  2*(2*G.K + 1)*sizeof(double), &can);
         const bool fused = tile_sums() && !L->t.alldd && can && !use_split(g, &a, &L->t) && !listm && nch >= 2*SQB_TILE*cap;
         /* the predictor at the last level: which children to leave out, and their tiers */
         if(pon){
@@ -795,7 +801,7 @@ extern "C" int sqb_dev_level_multi(const sqb_level_t *Ls, int n, sqb_acc_t *accs
         long c = maxch >> D;
         const size_t sm1 = 2*(2*(size_t)L.K + 1)*sizeof(double);
         int can0 = 0;
-        const long cap0 = grid_cap(g, which, sm1, &can0);
+        const long cap0 = grid_cap(g, which | SQB_ATTR_LEVEL, sm1, &can0);
         const long round = (cap0*SQB_TILE) >> D;
         if(can0 && round > 0 && c >= 2*round) c = (c/round)*round;
         ncb[k] = c; capk[k] = cap0; cank[k] = can0;

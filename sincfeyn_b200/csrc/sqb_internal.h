@@ -135,7 +135,14 @@ typedef struct {
 typedef struct {
     int regs, local_bytes, max_threads, blocks_per_sm;
     int fused;                    /* FP64 kernel: sums level tiles itself (level mode available) */
+    int sweeps;                   /* level kernel: passes over a batch's tiles (1, or 2: see SQB_SWEEPS) */
 } sqb_kattr_t;
+#define SQB_ATTR_LEVEL 4          /* attr(which | SQB_ATTR_LEVEL, ...): the FP64 level kernel's attributes */
+/* a launch that the FP64 level kernel runs: a level batch of cells (int8 coordinates) whose tiles come from
+ * the device queue, not in list mode */
+static inline bool sqb_level_launch(const sqb_eval_t *a){
+    return a->ninst > 0 && a->cells && a->esize == 1 && a->part && !a->sel && !a->sfin && !a->raw;
+}
 
 typedef struct {
     const char *name, *volkov;
@@ -143,8 +150,9 @@ typedef struct {
     int zlattice;                              /* 1: the variable is z itself (synthetic integrand) */
     void (*f64)(const sqb_eval_t *a, int grid, int block, size_t smem, void *stream);
     void (*dd)(const sqb_dd_t *a, int grid, int block, size_t smem, void *stream);
-    /* which: 0 FP64 kernel, 1 dd kernel, 2 contracted FP64 kernel; blocks_per_sm for this block size and
-     * dynamic shared memory; 0 if that kernel is not in the library */
+    /* which: 0 FP64 kernel, 1 dd kernel, 2 contracted FP64 kernel, with SQB_ATTR_LEVEL added: the FP64
+     * level kernel of that build; blocks_per_sm for this block size and dynamic shared memory; 0 if that
+     * kernel is not in the library */
     int (*attr)(int which, int block, size_t smem, sqb_kattr_t *out);
     /* the FP64 kernel compiled with contraction (-fmad=true: fused multiply-adds), from the graph's second
      * translation unit; NULL if the library was built without it */

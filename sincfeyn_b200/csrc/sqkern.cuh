@@ -43,6 +43,20 @@
 #ifndef SQB_MINB
 #define SQB_MINB 1            /* FP64 kernel: resident blocks per SM the register allocation must allow */
 #endif
+#ifndef SQB_LEVEL_KERNEL
+#ifdef SQB_FMA_TU
+#define SQB_LEVEL_KERNEL 1    /* the contracted unit: a level kernel beside the general one, both calling the point
+                                 function (sqb_fcall); the exact unit keeps one kernel with the function inlined */
+#else
+#define SQB_LEVEL_KERNEL 0
+#endif
+#endif
+#ifndef SQB_SWEEPS
+#define SQB_SWEEPS 1          /* level kernel: 2 = two sweeps over a batch's tiles, the children of cells that skip
+                                 the |.| sums first, then the others, so that the CTAs on an SM run one form of a
+                                 point function at a time (a large integrand's two forms do not fit the
+                                 instruction caches together); the reduce kernel then sums every tile */
+#endif
 #ifndef SQB_FUSE
 #define SQB_FUSE 1            /* FP64 kernel: level mode (tile sums in shared memory) compiled in; a kernel
                                  that spills its registers is built without it, keeping L1 for its stack */
@@ -84,13 +98,14 @@ __host__ __device__ __forceinline__ int sqb_table_words(const sqb_eval_t &a){
  * returns 0 for a child below the box, a child the predictor leaves out or, under a symmetry fold, a child
  * that is not the minimum of its orbit (driver/sum.c:405-416), else the point's multiplicity (the orbit
  * size; 1 without a fold) */
-template<int D, bool ORB = true>
+template<int D, bool ORB = true, int LV = 0>
 __device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const sqb_inst_t &I, const double *sX, const double *sW,
                                          long il, long ig, long *cell, double *sf, double *w){
     long c; int b;
-    if(a.cells){ c = il >> D; b = (int)(il & ((1L << D) - 1)); } else { c = il; b = 0; }
+    const bool cells = LV || a.cells;           /* the level kernel: cells of int8 coordinates */
+    if(cells){ c = il >> D; b = (int)(il & ((1L << D) - 1)); } else { c = il; b = 0; }
     *cell = c;
-    if(a.sfin){
+    if(!LV && a.sfin){
 #pragma unroll
         for(int d = 0; d < D; d++) sf[d] = a.sfin[ig*D + d];
         *w = 1.0;
@@ -99,7 +114,7 @@ __device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const sqb_inst_t &
     double ww = 1.0; bool in = true;
     int kk[D];
     const int K = I.K, st = I.st;
-    if(a.esize == 1){
+    if(LV || a.esize == 1){
         const signed char *p = (const signed char*)I.pts + c*(long)a.stride;
 #pragma unroll
         for(int d = 0; d < D; d++){
@@ -122,7 +137,7 @@ __device__ __forceinline__ int sqb_point(const sqb_eval_t &a, const sqb_inst_t &
     if(!in) return 0;
     if(a.cfl && (a.cfl[ig] & 1)) return 0;          /* left out by the predictor */
     if constexpr(!ORB) return 1;               /* list mode: the select pass has the orbit weight */
-    return a.cells && a.sym.n > 1 ? sqb_orbit<D>(a.sym, kk) : 1;
+    return cells && a.sym.n > 1 ? sqb_orbit<D>(a.sym, kk) : 1;
 }
 
 template<int D>
@@ -217,6 +232,21 @@ __device__ __forceinline__ void sqb_tile_flush(const sqb_eval_t &a, sqb_tile_acc
     }
 }
 
+/* The point function as a real call (contracted unit): its two forms (without and with the |.| sums) are
+ * compiled as functions apart from the callers' loop state, so that the level kernel and the general one
+ * share them instead of each inlining both (measured on the B200: as fast as the inlined function in the
+ * level kernel). */
+template<int D> struct sqb_pt { double s[D]; };
+struct sqb_fab { double f, ab; };
+template<class F, int D, int AB>
+__device__ __noinline__ sqb_fab sqb_fcall(const sqb_pt<D> p){
+    double sf[D];
+#pragma unroll
+    for(int d = 0; d < D; d++) sf[d] = p.s[d];
+    sqb_fab r; r.ab = 0; r.f = F::template f<double, AB>(sf, &r.ab);
+    return r;
+}
+
 /* The FP64 pass.  The CTAs take tiles of consecutive points in turn: tile b, b + gridDim.x, ... of one
  * batch, or, in a multi-instance launch, the next tile of the device counter queue (the tile's integral
  * from its position); SQB_TILE points per tile in level mode and in multi-instance launches, SQB_BLOCK
@@ -225,8 +255,13 @@ __device__ __forceinline__ void sqb_tile_flush(const sqb_eval_t &a, sqb_tile_acc
  * In level mode (a.part) each CTA also sums the tiles of its integrals that it is asked to (sqb_inst_t
  * fused): the children that need no fallback add v*pw and the rest into the thread's column of shared
  * memory; a tile with a fallback point, or of an integral the reduce kernel sums, is only flagged (a.tfb),
- * and the reduce kernel sums it after the double-double pass. */
-template<class F, int D>
+ * and the reduce kernel sums it after the double-double pass.
+ * LV = 1 is the level kernel: the same pass compiled for level batches alone (cells of int8 coordinates,
+ * tiles from the device queue, no list, no plain-form output), which leaves the other modes' code out of
+ * the kernel that runs almost every point (measured 3-4 % faster on the three-loop graphs); with
+ * SQB_SWEEPS = 2 it takes every tile twice, first for the children of cells that skip the |.| sums, then
+ * for the others.  LV = 0 runs every other launch. */
+template<class F, int D, int LV = 0>
 __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_constant__ sqb_eval_t a){
     extern __shared__ double sqb_sm[];
     __shared__ sqb_inst_t sI[SQB_MAXINST];
@@ -235,20 +270,24 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
 #if SQB_FUSE
     /* the tile sums' columns follow the tables in dynamic shared memory (level launches only) */
     sqb_tile_acc &ta = *(sqb_tile_acc*)(sqb_sm + sqb_table_words(a));
-    const bool lvl = a.part != NULL;
+    const bool lvl = LV || a.part != NULL;
 #else
     const bool lvl = false;
 #endif
+    constexpr int NSW = LV ? SQB_SWEEPS : 1;
     sqb_tables(a, sqb_sm, sI);
-    const bool multi = a.ninst > 0;
+    const bool multi = LV || a.ninst > 0;
+    const bool list = !LV && a.sel;
     const long n1 = multi ? 0 : (a.cells ? (a.n << D) : a.n);      /* one batch: its points */
     const long tl = (lvl || multi) ? SQB_TILE : SQB_BLOCK;          /* other modes: one point per thread per step */
-    const long nsel = a.sel ? (long)*a.nsel : 0;                    /* list mode (one integral, queue): its entries */
-    const long ntiles = a.sel ? (nsel + tl - 1)/tl : multi ? a.ntile : (n1 + tl - 1)/tl;
+    const long nsel = list ? (long)*a.nsel : 0;                     /* list mode (one integral, queue): its entries */
+    const long ntiles = list ? (nsel + tl - 1)/tl : multi ? a.ntile : (n1 + tl - 1)/tl;
     const int t = threadIdx.x;
-    long tile = blockIdx.x;
-    if(multi){ if(t == 0) s_tile = (long)atomicAdd(a.queue, 1ULL); __syncthreads(); tile = s_tile; }
-    while(tile < ntiles){
+    long q = blockIdx.x;                                            /* the work item: sweep*ntiles + tile */
+    if(multi){ if(t == 0) s_tile = (long)atomicAdd(a.queue, 1ULL); __syncthreads(); q = s_tile; }
+    while(q < NSW*ntiles){
+        const int sweep = NSW > 1 ? (int)(q/ntiles) : 0;
+        const long tile = NSW > 1 ? q - sweep*ntiles : q;
         int k = 0;
         if(multi){ if(t == 0) s_k = sqb_inst_at(a, tile*tl); __syncthreads(); k = s_k; }
         const sqb_inst_t &I = sI[k];
@@ -258,10 +297,10 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
         const double *sX = sqb_sm + I.toff, *sW = sX + (2*I.K + 1);
 #endif
         const long base = multi ? tile*tl - I.child0 : tile*tl;     /* the tile's first point in its integral */
-        const long n = multi ? (a.cells ? (I.n << D) : I.n) : n1;
+        const long n = multi ? ((LV || a.cells) ? (I.n << D) : I.n) : n1;
         const long off = multi ? I.child0 : 0;                       /* global index = local index + off */
 #if SQB_FUSE
-        const bool tsum = lvl && I.fused && !a.sel;
+        const bool tsum = lvl && I.fused && !list && NSW == 1;
         if(tsum){
             ta.S[0][t] = ta.S[1][t] = ta.A[t] = ta.dr[t] = ta.b1[0][t] = ta.b1[1][t] = ta.b2[0][t] = ta.b2[1][t] = 0;
             ta.ne[t] = ta.nsk[t] = ta.keep[t] = 0;
@@ -274,30 +313,42 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
         for(int j = 0; j < tl/SQB_BLOCK; j++){
             long il, i; int mw;
             long c; double sf[D], w;
-            if(a.sel){
-                const long q = tile*tl + (long)j*SQB_BLOCK + t;
-                if(q >= nsel) break;
-                const unsigned long long e = a.sel[q];
+            if(list){
+                const long e_ = tile*tl + (long)j*SQB_BLOCK + t;
+                if(e_ >= nsel) break;
+                const unsigned long long e = a.sel[e_];
                 il = i = (long)(e & ((1ULL << SQB_SEL_SHIFT) - 1));
-                sqb_point<D, false>(a, I, sX, sW, il, i, &c, sf, &w);
+                sqb_point<D, false, LV>(a, I, sX, sW, il, i, &c, sf, &w);
                 mw = (int)(e >> SQB_SEL_SHIFT);
             } else {
                 il = base + (long)j*SQB_BLOCK + t; i = il + off;
                 if(il >= n) break;
-                mw = sqb_point<D>(a, I, sX, sW, il, i, &c, sf, &w);
+                /* two sweeps: this child only in its cell's sweep (0: skips the |.| sums, 1: the others) */
+                if(NSW > 1 && (sqb_skip<D>(a, I, il >> D) ? 0 : 1) != sweep) continue;
+                mw = sqb_point<D, true, LV>(a, I, sX, sW, il, i, &c, sf, &w);
             }
             if(!mw){
                 a.v[i] = 0;
-                if(a.raw) a.ab[i] = 0; else a.stt[i] = 0;
+                if(!LV && a.raw) a.ab[i] = 0; else a.stt[i] = 0;
                 continue;
             }
             const int sk = sqb_skip<D>(a, I, c);
             const bool noab = sk && !a.abcheck;
             double ab = 0, f;
+#if SQB_LEVEL_KERNEL
+            {
+                sqb_pt<D> p;
+#pragma unroll
+                for(int d = 0; d < D; d++) p.s[d] = sf[d];
+                const sqb_fab r = noab ? sqb_fcall<F, D, 0>(p) : sqb_fcall<F, D, 1>(p);
+                f = r.f; ab = r.ab;
+            }
+#else
             if(noab) f = F::template f<double, 0>(sf, &ab);
             else     f = F::template f<double, 1>(sf, &ab);
+#endif
             const double fw = f*w;
-            if(a.raw){ a.v[i] = fw; a.ab[i] = ab*w; continue; }
+            if(!LV && a.raw){ a.v[i] = fw; a.ab[i] = ab*w; continue; }
             bool fallback;
             const double v = sqb_point_test(a, I, i, sk, noab, fw, ab*w, &fallback);
 #if SQB_FUSE
@@ -326,13 +377,13 @@ __global__ void __launch_bounds__(SQB_BLOCK, SQB_MINB) sqb_k_f64(const __grid_co
             __syncthreads();
         } else
 #endif
-        if(multi && a.tfb && !a.sel && t == 0) a.tfb[tile] = 1;      /* summed by the reduce kernel */
+        if(multi && a.tfb && !list && t == 0) a.tfb[tile] = 1;       /* summed by the reduce kernel */
         if(multi){
             __syncthreads();                                          /* every thread has read s_tile, s_k */
             if(t == 0) s_tile = (long)atomicAdd(a.queue, 1ULL);
             __syncthreads();
-            tile = s_tile;
-        } else tile += gridDim.x;
+            q = s_tile;
+        } else q += gridDim.x;
     }
 }
 
@@ -438,7 +489,16 @@ static int sqb_attr_of(K_ kernel, int block, size_t smem, sqb_kattr_t *o){
     if(cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return 0;
     if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, smem) != cudaSuccess) return 0;
     o->regs = fa.numRegs; o->local_bytes = (int)fa.localSizeBytes; o->max_threads = fa.maxThreadsPerBlock;
-    o->blocks_per_sm = nb; o->fused = 0; return 1;
+    o->blocks_per_sm = nb; o->fused = 0; o->sweeps = 1; return 1;
+}
+/* an FP64 (or dd) kernel's attributes; lv: the level kernel, which sums level tiles itself unless it sweeps
+ * twice */
+template<class K_>
+static int sqb_f64_attr(K_ kernel, int lv, int block, size_t smem, sqb_kattr_t *o){
+    if(!sqb_attr_of(kernel, block, smem, o)) return 0;
+    o->fused = SQB_FUSE && !(lv && SQB_SWEEPS > 1);
+    o->sweeps = lv ? SQB_SWEEPS : 1;
+    return 1;
 }
 template<class F, int D, int NP>
 static int sqb_split_attr(int P, int block, size_t smem, sqb_kattr_t *o){
@@ -486,14 +546,11 @@ struct F {                                                                      
 };                                                                                                 \
 }                                                                                                  \
 extern "C" void SQB_##NAME##_f64fma(const sqb_eval_t *a, int grid, int block, size_t smem, void *st){ \
-    sqb_k_f64<SQG_NS(NAME)::F, D><<<grid, block, smem, (cudaStream_t)st>>>(*a); }                  \
-extern "C" int SQB_##NAME##_attrfma(int block, size_t smem, sqb_kattr_t *o){                       \
-    cudaFuncAttributes fa; int nb = 0;                                                             \
-    if(cudaFuncGetAttributes(&fa, sqb_k_f64<SQG_NS(NAME)::F, D>) != cudaSuccess) return 0;         \
-    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sqb_k_f64<SQG_NS(NAME)::F, D>, block, smem) \
-       != cudaSuccess) return 0;                                                                   \
-    o->regs = fa.numRegs; o->local_bytes = (int)fa.localSizeBytes;                                 \
-    o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; o->fused = SQB_FUSE; return 1; }
+    if(sqb_level_launch(a)) sqb_k_f64<SQG_NS(NAME)::F, D, 1><<<grid, block, smem, (cudaStream_t)st>>>(*a); \
+    else sqb_k_f64<SQG_NS(NAME)::F, D, 0><<<grid, block, smem, (cudaStream_t)st>>>(*a); }           \
+extern "C" int SQB_##NAME##_attrfma(int lv, int block, size_t smem, sqb_kattr_t *o){               \
+    return lv ? sqb_f64_attr(sqb_k_f64<SQG_NS(NAME)::F, D, 1>, 1, block, smem, o)                  \
+              : sqb_f64_attr(sqb_k_f64<SQG_NS(NAME)::F, D, 0>, 0, block, smem, o); }
 #define SQ_GRAPH_SPLIT(NAME, VOLKOV, L, D, W, NP, FIX, NPARTS)                                      \
 SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                           \
 SQ_SPLIT_F(NAME)                                                                                   \
@@ -516,7 +573,7 @@ extern "C" void SQB_##NAME##_scale(const sqb_scale_t *a, int grid, int block, vo
 #define SQ_GRAPH_CORE(NAME, D)                                                                      \
 extern "C" void SQB_##NAME##_f64fma(const sqb_eval_t *, int, int, size_t, void *) __attribute__((weak)); \
 extern "C" void SQB_##NAME##_scale(const sqb_scale_t *, int, int, void *) __attribute__((weak));   \
-extern "C" int SQB_##NAME##_attrfma(int, size_t, sqb_kattr_t *) __attribute__((weak));             \
+extern "C" int SQB_##NAME##_attrfma(int, int, size_t, sqb_kattr_t *) __attribute__((weak));        \
 namespace SQG_NS(NAME) {                                                                           \
 struct F {                                                                                         \
     template<class R, int AB> static __device__ __forceinline__ R f(const R *sf, R *ab){           \
@@ -525,20 +582,17 @@ struct F {                                                                      
 template<> __device__ __forceinline__ sqdd F::f<sqdd, 1>(const sqdd *sf, sqdd *ab){                \
     return KD<sqdd, 1>::f_##NAME(sf, ab); }                                                        \
 static void f64(const sqb_eval_t *a, int grid, int block, size_t smem, void *st){                  \
-    sqb_k_f64<F, D><<<grid, block, smem, (cudaStream_t)st>>>(*a); }                                \
+    if(SQB_LEVEL_KERNEL && sqb_level_launch(a))                                                    \
+        sqb_k_f64<F, D, SQB_LEVEL_KERNEL><<<grid, block, smem, (cudaStream_t)st>>>(*a);            \
+    else sqb_k_f64<F, D, 0><<<grid, block, smem, (cudaStream_t)st>>>(*a); }                        \
 static void dd(const sqb_dd_t *a, int grid, int block, size_t smem, void *st){                     \
     sqb_k_dd<F, D><<<grid, block, smem, (cudaStream_t)st>>>(*a); }                                 \
 static int attr(int which, int block, size_t smem, sqb_kattr_t *o){                                \
-    if(which == 2) return SQB_##NAME##_attrfma ? SQB_##NAME##_attrfma(block, smem, o) : 0;          \
-    cudaFuncAttributes fa; int nb = 0;                                                             \
-    cudaError_t e = which ? cudaFuncGetAttributes(&fa, sqb_k_dd<F, D>)                             \
-                          : cudaFuncGetAttributes(&fa, sqb_k_f64<F, D>);                           \
-    if(e != cudaSuccess) return 0;                                                                 \
-    e = which ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sqb_k_dd<F, D>, block, smem)    \
-              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sqb_k_f64<F, D>, block, smem);  \
-    if(e != cudaSuccess) return 0;                                                                 \
-    o->regs = fa.numRegs; o->local_bytes = (int)fa.localSizeBytes;                                 \
-    o->max_threads = fa.maxThreadsPerBlock; o->blocks_per_sm = nb; o->fused = SQB_FUSE; return 1; } \
+    const int lv = (which & SQB_ATTR_LEVEL) != 0; which &= ~SQB_ATTR_LEVEL;                        \
+    if(which == 2) return SQB_##NAME##_attrfma ? SQB_##NAME##_attrfma(lv, block, smem, o) : 0;      \
+    if(which == 1) return sqb_f64_attr(sqb_k_dd<F, D>, 0, block, smem, o);                         \
+    return SQB_LEVEL_KERNEL && lv ? sqb_f64_attr(sqb_k_f64<F, D, SQB_LEVEL_KERNEL>, 1, block, smem, o) \
+                                  : sqb_f64_attr(sqb_k_f64<F, D, 0>, 0, block, smem, o); }         \
 }
 #define SQ_GRAPH(NAME, VOLKOV, L, D, W, NP, FIX)                                                    \
 SQ_GRAPH_CORE(NAME, D)                                                                             \
