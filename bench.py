@@ -194,14 +194,14 @@ def run_mixed(args, sq, L):
     refinement levels in shared launches over the four integrals, tiles from a device queue); device time
     of each whole batch, points/s, and the runs' values, which must be identical (each integral's
     arithmetic does not depend on the schedule).  The tuner runs a calibration sample (every 8th graph's
-    four integrals) once per candidate (workers, grouped or not) and picks the fastest."""
+    four integrals) twice per candidate (workers, grouped or not) and picks the fastest."""
     import torch
     jobs = mixed_jobs(sq)
     for g in sorted({j[0] for j in jobs}):
         sq.preload(g)
     graphs = sorted({j[0] for j in jobs})
     sample = [j for j in jobs if j[0] in graphs[::8]]
-    # warm-up and tuning: the calibration sample once per candidate
+    # warm-up and tuning: the calibration sample twice per candidate
     rates = {}
     best, best_rate = None, -1.0
     for grp in (0, 1):
@@ -459,7 +459,7 @@ def main():
     t_load = time.perf_counter() - t_load
     # cost estimate for the largest-first order: children per cell times flops per point
     jobs = [(g, H, N_PTS, EPS, -1, float(2**D_OF[g])*sq.flops(g, 1)) for g in mine]
-    # the batch tuner (untimed): every 4th integral of this rank's share once per candidate worker count;
+    # the batch tuner (untimed): every 4th integral of this rank's share twice per candidate worker count;
     # the sample leaves out the costliest integral, which alone would set its time whatever the count
     top = max(j[5] for j in jobs)
     workers, tune_rates = sq.batch_tune([j for j in jobs if j[5] < top][::4], BATCH_CANDIDATES, device=local)

@@ -158,8 +158,9 @@ int  sqb_hsum_batch(const sqb_job_t *jobs, int n, const sqb_opts_t *o, int worke
  * (ckpt_every > 0), the predictor, the all-dd form or the pass split runs its integrals one after another.
  * Returns 0, or the number of failed jobs (sqb_error() names the first). */
 int  sqb_hsum_group(const sqb_job_t *jobs, int n, const sqb_opts_t *o, sqb_result_t *res, int *rcs);
-/* the batch tuner: runs the calibration jobs once per candidate worker count, rate[c] = evaluated points
- * per second of device time; *best = the fastest candidate.  Returns 0 or a batch error. */
+/* the batch tuner: runs the calibration jobs twice per candidate worker count, the candidates in turn, rate[c]
+ * = the better of the two runs' evaluated points per second of device time (the first run of a worker count
+ * also pays its workers' first allocations); *best = the fastest candidate.  Returns 0 or a batch error. */
 int  sqb_batch_tune(const sqb_job_t *jobs, int n, const sqb_opts_t *o, const int *cand, int ncand, double *rate,
                     int *best);
 

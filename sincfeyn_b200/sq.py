@@ -263,8 +263,8 @@ def hsum_group(jobs, **opts):
 
 
 def batch_tune(jobs, candidates=(1, 2, 4, 6, 8), **opts):
-    """The batch tuner (sqb_batch_tune): runs the calibration jobs once per candidate worker count;
-    returns (best worker count, {count: points per second of device time})."""
+    """The batch tuner (sqb_batch_tune): runs the calibration jobs twice per candidate worker count;
+    returns (best worker count, {count: points per second of device time, the better run})."""
     arr = _jobs(jobs)
     cand = (C.c_int * len(candidates))(*candidates)
     rate = (C.c_double * len(candidates))()
