@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <omp.h>
 #include <chrono>
+#include <future>
 #include "sqb_rt.h"
 #include "sincfeyn_b200.h"
 
@@ -156,13 +157,25 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
     /* the grow's device tables are released on every return, an error included, so that a failed
      * integral leaves its memory to the next one */
     struct End { ~End(){ sqb_grow_end(); } } end_of_grow;
-    std::vector<double> v; std::vector<unsigned char> stt, cls;
+    std::vector<unsigned char> stt;
     ksum ks; double a = 0, x1 = 0, x2 = 0, dr = 0, gshs = 0; long ne = 0, gshn = 0, nkeep = 0;
     double te = 0, th = 0, tx = 0; int nfr = 0; const double tg0 = now();    /* phase times (verbose) */
+    /* A frontier's order-dependent sums that its expansion does not need (the Neumaier S, the shell, drop
+     * and shadow sums) run on a helper task while the device expands the frontier and evaluates the next;
+     * the tasks run one frontier after another (each waits for its predecessor), each over its frontier in
+     * point order, so every sum is the in-line one bit for bit.  Only the |v| sum that sets the threshold
+     * stays in line.  Values and shell classes alternate between two buffers; every return joins the
+     * tasks first. */
+    std::vector<double> vb[2]; std::vector<unsigned char> cb[2];
+    std::shared_future<void> fut[2], last;
+    struct Join { std::shared_future<void> &f; ~Join(){ if(f.valid()) f.wait(); } } join{last};
     for(;;){
         const sqb_pt_t *pts; const unsigned char *skip;
         const long n = sqb_grow_frontier(&pts, &skip);
         if(n <= 0) break;
+        const int b = nfr & 1;
+        if(fut[b].valid()) fut[b].wait();          /* the task two frontiers back read this buffer */
+        std::vector<double> &v = vb[b]; std::vector<unsigned char> &cls = cb[b];
         v.resize(n); stt.resize(n); cls.resize(n);
         const double *vd; const unsigned char *sd;
         const double t0 = now();
@@ -176,12 +189,20 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
         const double t1 = now(); te += t1 - t0; nfr++;
         ne += n;
         /* the frontier's sums in point order, then its threshold (driver/sumkey.h:225-245) */
-        for(long i = 0; i < n; i++){ ks.add(v[i]*pw); a += fabs(v[i])*pw; }
+        for(long i = 0; i < n; i++) a += fabs(v[i])*pw;
         const double thr = eps_rel*a;
-        for(long i = 0; i < n; i++){
-            const double w = fabs(v[i])*pw;
-            if(cls[i] & 2) x1 += w; else if(cls[i] & 4) x2 += w;
-            if(!(fabs(v[i]) >= thr)){ dr += w; gshs += v[i]*pw; gshn++; }
+        {
+            const std::shared_future<void> prev = last;
+            last = fut[b] = std::async(std::launch::async, [&, b, n, thr, prev]{
+                if(prev.valid()) prev.wait();
+                const double *vv = vb[b].data(); const unsigned char *cc = cb[b].data();
+                for(long i = 0; i < n; i++) ks.add(vv[i]*pw);
+                for(long i = 0; i < n; i++){
+                    const double w = fabs(vv[i])*pw;
+                    if(cc[i] & 2) x1 += w; else if(cc[i] & 4) x2 += w;
+                    if(!(fabs(vv[i]) >= thr)){ dr += w; gshs += vv[i]*pw; gshn++; }
+                }
+            }).share();
         }
         long nk = 0, nn = 0;
         const double t2 = now(); th += t2 - t1;
@@ -189,6 +210,7 @@ static int grow(Run &R, int lev, double eps_rel, GrowOut *go, sqb_pt_t **dilated
         tx += now() - t2;
         nkeep += nk;
     }
+    if(last.valid()) last.wait();                  /* every frontier's sums are in */
     const double tg1 = now();
     /* the final threshold, driver/sumkey.h:399-401 */
     const double thr = eps_rel*a;
