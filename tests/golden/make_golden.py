@@ -221,8 +221,11 @@ def mixed2():
 
 VP4_H = ((1.0, 97), (0.9, 107))
 # a dimension-stratified sample of kernels/v4 and kernels/w4 (D = 6, 7, 8, 9; the cheapest D = 9 graph at
-# h = 2.0), and the lepton-loop sets I(a), I(b), I(c) of docs/LEPTON_LOOPS.md:5-17
-VP4_SAMPLE = {1.0: ['w4_00Sc', 'v4_00', 'w4_00Sm', 'w4_00Vm', 'w4_0iSc', 'w4_0iSm', 'w4_0iVm', 'v4_02', 'v4_14'],
+# h = 2.0), the lepton-loop sets I(a), I(b), I(c) of docs/LEPTON_LOOPS.md:5-17, and two large integrands with
+# many cells near the fallback at h = 1.0 (v4_65, w4_04Sm: 38 % and 21 % of their evaluations with the |.|
+# sums), whose contracted level kernel takes each batch in two sweeps
+VP4_SAMPLE = {1.0: ['w4_00Sc', 'v4_00', 'w4_00Sm', 'w4_00Vm', 'w4_0iSc', 'w4_0iSm', 'w4_0iVm', 'v4_02', 'v4_14',
+                    'v4_65', 'w4_04Sm'],
               0.9: ['w4_00Sc', 'v4_00', 'w4_00Sm', 'w4_0iSc', 'w4_0iSm', 'v4_02']}     # D = 6..8 at h = 0.9
 VP4_FILE = os.path.join(OUT, 'vp4_sample.json')
 

@@ -1,7 +1,8 @@
 """The four-loop lepton-loop kernels (kernels/v4, kernels/w4) at h = 1.0 (N = 97) and h = 0.9 (N = 107),
 eps = 1e-12, against the reference CPU run of a dimension-stratified sample (D = 6, 7, 8 and 9;
-tests/golden/vp4_sample.json: -ffp-contract=off build, SINCQED_SYM=0, SINCQED_KEEPBT=1), and the
-lepton-loop sets with exactly known values (docs/LEPTON_LOOPS.md:5-17) (GPU).
+tests/golden/vp4_sample.json: -ffp-contract=off build, SINCQED_SYM=0, SINCQED_KEEPBT=1; with v4_65 and
+w4_04Sm, whose contracted level kernel takes each batch in two sweeps over many cells near the fallback),
+and the lepton-loop sets with exactly known values (docs/LEPTON_LOOPS.md:5-17) (GPU).
 
   * every graph of the sample, as written (fma = 0): the same evaluation count, the value within 1e-11
     relative (the four-loop tolerance); contracted (the default form, the sample as one batch): the
